@@ -1,0 +1,391 @@
+"""Benchmark of the estimation epoch on B200.
+
+One step = one estimation epoch (run_epoch) of one scenario: forward
+propagation, measurement products and residuals, reference-mode derivation
+and the Adam update, over all steps of every beat.
+
+Workload (default): 20x20x20 cuboid (8,000 voxels, 24,000 states), 2,000
+steps at 2 kHz, 37 triaxial sensors (111 rows), one beat, random 5^3
+zero-gain block, 1% Gaussian measurement noise, Adam lr 1e-3, gains and
+all-pass coefficients both trained (textbook derivative). Inputs are seeded
+synthetic arrays of that shape.
+
+Timing: W untimed warm-up epochs, then K epochs each bracketed by CUDA events
+on the library's stream, with a >L2 buffer written between epochs (not
+timed). Multi-GPU (torchrun): each rank runs its own scenario (different
+seed), no data-path collective; time = max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "scenario-epochs/s and voxel-steps/s, chosen vs plain GPU form at stated grad tol"
+UNIT = "scenario-epochs/s"
+WORKLOAD = "cuboid20"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default=WORKLOAD)
+    p.add_argument("--cpu-steps", type=int, default=200, help="steps of the bounded CPU sample")
+    return p.parse_args()
+
+
+def algorithm_config(alg):
+    return alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False,
+                         ap_derivative=alg.APDerivative.Textbook)
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+# ----------------------------------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------- CPU
+
+
+def cpu_sample(scn, cpu_steps: int, threads: int = 1):
+    """The CPU restatement (oracle/, reference loop order, f32) on the first `cpu_steps`
+    steps of the workload, `threads` independent replicas in parallel (one scenario per
+    thread, as the reference scheduler runs scenarios). Returns (scenario-epochs/s, seconds)."""
+    import numpy as np
+
+    import oracle
+
+    T = min(cpu_steps, scn.num_steps)
+    cfg = oracle.algo(optimizer=1, learning_rate=1e-3, freeze_delays=0)
+    epochs = []
+    for _ in range(threads):
+        epochs.append(oracle.OracleEpoch(
+            scn.model.gains, scn.model.output_state_indices, scn.model.coefs, scn.model.delays,
+            scn.model.initial_delays, scn.measurement_matrix, scn.control_matrix, scn.control_function[:T],
+            np.ascontiguousarray(scn.measurements[:, :T]), num_batch_slots=1))
+    ts = [threading.Thread(target=e.run_epoch, args=(cfg,)) for e in epochs]
+    t0 = time.perf_counter()
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    dt = time.perf_counter() - t0
+    # each replica did T/scn.num_steps of one full epoch
+    return threads * (T / scn.num_steps) / dt, dt
+
+
+def reference_arm(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    from cardiotrust_b200 import scenario as sc
+
+    import oracle
+
+    oracle.build()
+    scn = sc.build(sc.workload_spec(args.workload, seed=0))
+    # ground truth on the CPU restatement: forward of the truth model on the sampled steps
+    T = min(args.cpu_steps, scn.num_steps)
+    o = oracle.OracleEpoch(scn.truth.gains, scn.truth.output_state_indices, scn.truth.coefs, scn.truth.delays,
+                           scn.truth.initial_delays, scn.measurement_matrix, scn.control_matrix,
+                           scn.control_function[:T])
+    import numpy as np
+
+    y = o.simulate()
+    full = np.zeros((scn.num_beats, scn.num_steps, scn.num_sensors), np.float32)
+    full[:, :T] = y
+    scn.measurements = full
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    for _ in range(args.warmup):
+        pass  # the CPU path has no warm-up effects worth a full sample; warm-up steps are not run
+    # per-step sample sized so K steps stay within a few minutes
+    per_step = max(20, min(args.cpu_steps, (10 * scn.num_steps) // max(1, args.steps * 10)))
+    vals = []
+    t_all = 0.0
+    for _ in range(args.steps):
+        v, dt = cpu_sample(scn, per_step, threads=cores)
+        vals.append(v)
+        t_all += dt
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1000.0 / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.workload}: 20x20x20 cuboid, 24000 states, T=2000, 111 sensor rows, 1 beat, "
+                               "Adam lr 1e-3, gains+coefficients", "parallelism": f"{cores} CPU threads, one scenario each"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"first {per_step} of {scn.num_steps} steps of one epoch per thread, scaled by "
+                                   f"{scn.num_steps / per_step:.0f}; later steps are slower on x86 (subnormal states), so "
+                                   "this overstates CPU throughput"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------------------- GPU
+
+
+def gpu_arm(args):
+    import numpy as np
+    import torch
+
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    from cardiotrust_b200 import algorithm as alg
+    from cardiotrust_b200 import scenario as sc
+
+    stream = torch.cuda.current_stream()
+    ctx = alg.Context(local_rank, stream=stream.cuda_stream)
+    scn = sc.build(sc.workload_spec(args.workload, seed=rank))
+    # ground truth with the CUDA forward (Simulation::run reuses the prediction path)
+    truth = alg.EpochEngine.from_scenario(ctx, scn, truth=True)
+    y = truth.simulate()
+    truth.close()
+    rng = np.random.default_rng(scn.spec.seed + 7919)
+    sigma = scn.spec.noise_fraction * float(np.sqrt(np.mean(y.astype(np.float64) ** 2)))
+    scn.measurements = (y + rng.normal(0.0, sigma, size=y.shape)).astype(np.float32)
+
+    cfg = algorithm_config(alg)
+    total_epochs = args.warmup + 3 * args.steps + 4
+    eng = alg.EpochEngine.from_scenario(ctx, scn, num_batch_slots=total_epochs, algorithm=cfg)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    V, T, B = scn.num_voxels, scn.num_steps, scn.num_beats
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+
+    bi = 0
+    for _ in range(args.warmup):
+        bi = eng.run_epoch(bi, sync=True)
+    barrier()
+
+    # ---- device-resident timed region
+    launches0 = eng.kernel_launches()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.random_(0, 255)
+        ev[k][0].record(stream)
+        bi = eng.run_epoch(bi, sync=False)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    eng.sync()
+    clock = clocks.stop()
+    launches = (eng.kernel_launches() - launches0) // args.steps
+    ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps / (total_ms / 1000.0)
+    barrier()
+
+    # ---- end to end through the C ABI with host buffers (pinned), copies inside the timed region
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    h_gains, h_coefs = pin(eng.read("gains")), pin(eng.read("coefs"))
+    h_delays, h_meas = pin(eng.read("delays")), pin(scn.measurements)
+    out_gains, out_coefs, out_delays = pin(np.empty_like(h_gains)), pin(np.empty_like(h_coefs)), pin(np.empty_like(h_delays))
+    out_loss = pin(np.empty(eng.dims["NB"], np.float32))
+    h2d = h_gains.nbytes + h_coefs.nbytes + h_delays.nbytes + h_meas.nbytes
+    d2h = out_gains.nbytes + out_coefs.nbytes + out_delays.nbytes + 4 * eng.dims["NB"]
+    e2e_steps = max(3, args.steps // 2)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        eng.write("gains", h_gains)
+        eng.write("coefs", h_coefs)
+        eng.write("delays", h_delays)
+        eng.write("measurements_actual", h_meas)
+        bi = eng.run_epoch(bi, sync=True)
+        eng.read_into("gains", out_gains)
+        eng.read_into("coefs", out_coefs)
+        eng.read_into("delays", out_delays)
+        eng.read_into("loss_batch", out_loss)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * e2e_steps / e2e_s
+    barrier()
+
+    # ---- per-phase device time (CUDA events on the library stream) for the roofline
+    eng.set_profiling(True)
+    for _ in range(args.steps):
+        flush.random_(0, 255)
+        bi = eng.run_epoch(bi, sync=False)
+    prof = eng.read_profile()
+    eng.set_profiling(False)
+    peaks = {}
+    pp = ROOT / "MEASURED_PEAKS.json"
+    if pp.exists():
+        peaks = json.loads(pp.read_text())
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    S = 3 * V
+    phase_ms = {k: v[0] / args.steps for k, v in prof.items()}
+    dominant = max(phase_ms, key=phase_ms.get)
+    # algorithmic bytes per launch (per beat): propagation 601*S per step; derivative sweep 740*S per step
+    algo_bytes = {"forward": 601.0 * S * T, "derive": 740.0 * S * T}
+    rl_kernel = dominant if dominant in algo_bytes else "forward"
+    launches_of = max(1, prof[rl_kernel][1] // args.steps)
+    per_launch_ms = phase_ms[rl_kernel] / launches_of
+    achieved = algo_bytes[rl_kernel] / (per_launch_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": rl_kernel, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "peak_source": peak_src, "traffic": None,
+                "algorithmic_bytes_per_launch": algo_bytes[rl_kernel], "launch_ms": per_launch_ms}
+
+    # ---- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1:
+        try:
+            import oracle
+
+            oracle.build()
+            v, dt = cpu_sample(scn, args.cpu_steps, threads=1)
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": f"first {min(args.cpu_steps, T)} of {T} steps of one epoch (single thread, reference "
+                             f"loop order), scaled by {T / min(args.cpu_steps, T):.0f}; {dt:.1f} s; later steps are "
+                             "slower on x86 (subnormal states), so this overstates CPU throughput"}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "port", "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {
+                "workload": f"{args.workload}: 20x20x20 cuboid, {V} voxels, {S} states, T={T}, "
+                            f"{scn.num_sensors} sensor rows, {B} beat, Adam lr 1e-3, gains+coefficients (textbook)",
+                "voxels": V, "states": S, "steps_per_epoch": T, "beats": B, "sensor_rows": scn.num_sensors,
+                "grad_mode": "reference", "precision": "fp32",
+                "l2": "256 MB buffer written between timed epochs (not timed)",
+                "parallelism": f"replicas x{world}",
+            },
+            "voxel_steps_per_s": value * V * T * B,
+            "phase_ms": phase_ms,
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "clocks": clock,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    ctx.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

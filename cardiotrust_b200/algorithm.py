@@ -1,0 +1,352 @@
+"""Host-side mirror of the reference estimation API over the CUDA library.
+
+Reference interface (paths relative to the crate root):
+
+* ``run_epoch(results: &mut Results, batch_index: &mut usize, data: &Data,
+  config: &Algorithm) -> anyhow::Result<()>``  — src/core/algorithm.rs:124-129
+* ``Algorithm`` (the fields the epoch reads)   — src/core/config/algorithm.rs:25-85
+* ``Results { metrics, estimations, derivatives, model }`` — src/core/scenario/results.rs:28-34
+* ``Optimizer {Sgd, Adam}``                     — src/core/algorithm/refinement.rs:8-12
+* ``APDerivative {Simple, Textbook}``           — src/core/config/algorithm.rs:17-21
+
+Every call goes through ``include/cardiotrust_cuda.h``; errors surface as
+:class:`~cardiotrust_b200._lib.CtError` (the counterpart of ``anyhow::Error``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import enum
+from types import SimpleNamespace
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import CtError, check, fptr, iptr, lib
+
+
+class Optimizer(enum.IntEnum):
+    Sgd = 0
+    Adam = 1
+
+
+class APDerivative(enum.IntEnum):
+    Simple = 0
+    Textbook = 1
+
+
+class GradMode(enum.IntEnum):
+    Reference = 0
+
+
+class Precision(enum.IntEnum):
+    Fp32 = 0
+
+
+@dataclasses.dataclass
+class Algorithm:
+    """Algorithm config with the reference defaults (config/algorithm.rs:59-85)."""
+
+    optimizer: Optimizer = Optimizer.Sgd
+    epochs: int = 10
+    batch_size: int = 0
+    learning_rate: float = 200.0
+    mse_strength: float = 1.0
+    slow_down_stregth: float = 0.0  # read by nothing on the epoch path (update.rs:163-167)
+    maximum_regularization_strength: float = 1.0
+    maximum_regularization_threshold: float = 1.01
+    difference_regularization_strength: float = 0.0
+    smoothness_regularization_strength: float = 0.0
+    freeze_gains: bool = False
+    freeze_delays: bool = True
+    ap_derivative: APDerivative = APDerivative.Textbook
+
+    def to_ct(self) -> _lib.CtAlgorithm:
+        a = _lib.CtAlgorithm()
+        a.optimizer = int(self.optimizer)
+        a.ap_derivative = int(self.ap_derivative)
+        a.freeze_gains = int(bool(self.freeze_gains))
+        a.freeze_delays = int(bool(self.freeze_delays))
+        a.batch_size = int(self.batch_size)
+        a.learning_rate = float(self.learning_rate)
+        a.mse_strength = float(self.mse_strength)
+        a.maximum_regularization_strength = float(self.maximum_regularization_strength)
+        a.maximum_regularization_threshold = float(self.maximum_regularization_threshold)
+        a.difference_regularization_strength = float(self.difference_regularization_strength)
+        a.smoothness_regularization_strength = float(self.smoothness_regularization_strength)
+        return a
+
+
+class Context:
+    """A device and the stream all work is issued on (GPU::new, gpu.rs:31-64)."""
+
+    def __init__(self, device: int = 0, stream: Optional[int] = None):
+        self._h = ctypes.c_void_p()
+        check(lib().ct_ctx_create(int(device), ctypes.c_void_p(stream) if stream else None, ctypes.byref(self._h)))
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        check(lib().ct_ctx_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def close(self) -> None:
+        if self._h:
+            lib().ct_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a), dtype=np.float32)
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a), dtype=np.int32)
+
+
+class EpochEngine:
+    """One scenario's model, estimations, derivatives and metrics in GPU memory."""
+
+    def __init__(
+        self,
+        ctx: Context,
+        *,
+        gains,
+        output_state_indices,
+        coefs,
+        delays,
+        initial_delays,
+        measurement_matrix,
+        control_matrix,
+        control_function,
+        measurements=None,
+        num_batch_slots: int = 1,
+        algorithm: Optional[Algorithm] = None,
+    ):
+        self.ctx = ctx
+        self.algorithm = algorithm or Algorithm()
+        H = _f32(measurement_matrix)
+        if H.ndim != 3:
+            raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, "measurement_matrix must be [beats, sensors, states]")
+        B, M, S = H.shape
+        u = _f32(control_function)
+        keep = dict(
+            gains=_f32(gains),
+            osi=_i32(output_state_indices),
+            coefs=_f32(coefs),
+            delays=_i32(delays),
+            init=_f32(initial_delays),
+            H=H,
+            ctrl=_f32(control_matrix),
+            u=u,
+            meas=None if measurements is None else _f32(measurements),
+        )
+        V = S // 3
+        expect = dict(gains=(S, 78), osi=(S, 78), coefs=(V, 26), delays=(V, 26), init=(V, 26), ctrl=(S,), u=(u.shape[0],))
+        for k, shp in expect.items():
+            if tuple(keep[k].shape) != shp:
+                raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, f"{k} has shape {keep[k].shape}, expected {shp}")
+        if keep["meas"] is not None and keep["meas"].shape != (B, u.shape[0], M):
+            raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, f"measurements have shape {keep['meas'].shape}")
+        d = _lib.CtScenarioDesc()
+        d.num_states, d.num_sensors, d.num_steps, d.num_beats = S, M, u.shape[0], B
+        d.num_batch_slots = int(num_batch_slots)
+        d.gains = fptr(keep["gains"])
+        d.output_state_indices = iptr(keep["osi"])
+        d.coefs = fptr(keep["coefs"])
+        d.delays = iptr(keep["delays"])
+        d.initial_delays = fptr(keep["init"])
+        d.measurement_matrix = fptr(H)
+        d.control_matrix = fptr(keep["ctrl"])
+        d.control_function = fptr(u)
+        d.measurements = fptr(keep["meas"]) if keep["meas"] is not None else None
+        self._h = ctypes.c_void_p()
+        ca = self.algorithm.to_ct()
+        check(lib().ct_scenario_create(ctx.handle, ctypes.byref(d), ctypes.byref(ca), ctypes.byref(self._h)))
+        self.dims = dict(S=S, V=V, M=M, T=u.shape[0], B=B, NB=int(num_batch_slots))
+
+    # -- parameters
+    def set_algorithm(self, algorithm: Algorithm) -> None:
+        self.algorithm = algorithm
+        ca = algorithm.to_ct()
+        check(lib().ct_set_algorithm(self._h, ctypes.byref(ca)))
+
+    def set_freeze(self, freeze_gains: bool, freeze_delays: bool) -> None:
+        check(lib().ct_set_freeze(self._h, int(freeze_gains), int(freeze_delays)))
+
+    def set_learning_rate(self, lr: float) -> None:
+        check(lib().ct_set_learning_rate(self._h, float(lr)))
+
+    # -- work
+    def run_epoch(self, batch_index: int = 0, beat_order=None, grad_mode=GradMode.Reference,
+                  precision=Precision.Fp32, sync: bool = True) -> int:
+        bi = ctypes.c_int64(int(batch_index))
+        order = None if beat_order is None else _i32(beat_order)
+        check(lib().ct_run_epoch(self._h, ctypes.byref(bi), None if order is None else iptr(order), int(grad_mode),
+                                 int(precision)))
+        if sync:
+            self.sync()
+        return bi.value
+
+    def simulate(self, with_states: bool = False):
+        D = self.dims
+        y = np.empty((D["B"], D["T"], D["M"]), dtype=np.float32)
+        x = np.empty((D["T"], D["S"]), dtype=np.float32) if with_states else None
+        check(lib().ct_simulate(self._h, fptr(y), fptr(x) if x is not None else None))
+        return (y, x) if with_states else y
+
+    def sync(self) -> None:
+        check(lib().ct_sync(self._h))
+
+    def kernel_launches(self) -> int:
+        n = ctypes.c_int64()
+        check(lib().ct_kernel_launches(self._h, ctypes.byref(n)))
+        return n.value
+
+    def set_profiling(self, enable: bool) -> None:
+        check(lib().ct_set_profiling(self._h, int(enable)))
+
+    def read_profile(self) -> dict:
+        """{phase: (device ms, kernel launches)} accumulated since profiling was enabled."""
+        n = len(_lib.PHASES)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int64 * n)()
+        check(lib().ct_read_profile(self._h, ms, cnt))
+        return {p: (ms[i], cnt[i]) for i, p in enumerate(_lib.PHASES)}
+
+    # -- fields
+    def read(self, name: str) -> np.ndarray:
+        code, dtype, shape = _lib.FIELDS[name]
+        D = self.dims
+        out = np.empty(shape(D["S"], D["V"], D["M"], D["T"], D["B"], D["NB"]), dtype=dtype)
+        check(lib().ct_read_field(self._h, code, out.ctypes.data_as(ctypes.c_void_p), out.nbytes))
+        return out
+
+    def read_into(self, name: str, out: np.ndarray) -> np.ndarray:
+        """Read a field into a caller-owned C-contiguous array (e.g. pinned host memory)."""
+        code, dtype, shape = _lib.FIELDS[name]
+        D = self.dims
+        want = shape(D["S"], D["V"], D["M"], D["T"], D["B"], D["NB"])
+        if out.shape != want or out.dtype != np.dtype(dtype) or not out.flags.c_contiguous:
+            raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, f"{name} needs a C-contiguous {dtype} array of shape {want}")
+        check(lib().ct_read_field(self._h, code, out.ctypes.data_as(ctypes.c_void_p), out.nbytes))
+        return out
+
+    def write(self, name: str, value) -> None:
+        code, dtype, shape = _lib.FIELDS[name]
+        D = self.dims
+        arr = np.ascontiguousarray(np.asarray(value), dtype=dtype)
+        want = shape(D["S"], D["V"], D["M"], D["T"], D["B"], D["NB"])
+        if arr.shape != want:
+            raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, f"{name} has shape {arr.shape}, expected {want}")
+        check(lib().ct_write_field(self._h, code, arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes))
+
+    def close(self) -> None:
+        if self._h:
+            lib().ct_scenario_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @classmethod
+    def from_scenario(cls, ctx: Context, scn, *, truth: bool = False, num_batch_slots: int = 1,
+                      algorithm: Optional[Algorithm] = None) -> "EpochEngine":
+        p = scn.truth if truth else scn.model
+        return cls(
+            ctx,
+            gains=p.gains,
+            output_state_indices=p.output_state_indices,
+            coefs=p.coefs,
+            delays=p.delays,
+            initial_delays=p.initial_delays,
+            measurement_matrix=scn.measurement_matrix,
+            control_matrix=scn.control_matrix,
+            control_function=scn.control_function,
+            measurements=scn.measurements,
+            num_batch_slots=num_batch_slots,
+            algorithm=algorithm,
+        )
+
+
+# ------------------------------------------------------------------------------------------
+# Reference-shaped wrappers
+
+
+@dataclasses.dataclass
+class Data:
+    """``Data.simulation.measurements`` [beats, steps, sensors] (data.rs:13-15)."""
+
+    measurements: np.ndarray
+
+
+class Results:
+    """``Results`` (results.rs:28-34) whose arrays live on the GPU; attribute groups read on access."""
+
+    def __init__(self, engine: EpochEngine):
+        self.engine = engine
+        self._data_id = None
+
+    def _group(self, names):
+        return SimpleNamespace(**{n: self.engine.read(n) for n in names})
+
+    @property
+    def metrics(self):
+        return self._group(
+            ["loss", "loss_mse", "loss_maximum_regularization", "loss_batch", "loss_mse_batch",
+             "loss_maximum_regularization_batch"]
+        )
+
+    @property
+    def estimations(self):
+        return self._group(
+            ["ap_outputs_now", "ap_outputs_last", "system_states", "measurements", "residuals", "average_delays"]
+        )
+
+    @property
+    def derivatives(self):
+        return self._group(
+            ["grad_gains", "grad_coefs", "coefs_fir", "coefs_iir", "mapped_residuals", "maximum_regularization",
+             "maximum_regularization_sum", "adam_step"]
+        )
+
+    @property
+    def ap_params(self):
+        return self._group(["gains", "coefs", "delays"])
+
+
+class BatchIndex:
+    """Mutable batch cursor, the ``&mut usize`` of run_epoch."""
+
+    def __init__(self, value: int = 0):
+        self.value = int(value)
+
+
+def run_epoch(results: Results, batch_index: BatchIndex, data: Data, config: Algorithm, beat_order=None) -> None:
+    """One estimation epoch (algorithm.rs:124-281) on the GPU.
+
+    ``beat_order`` fixes the beat visiting order; None uses the library's
+    seeded shuffle (the reference shuffles with an unseeded generator).
+    """
+    eng = results.engine
+    if results._data_id != id(data):
+        eng.write("measurements_actual", data.measurements)
+        results._data_id = id(data)
+    eng.set_algorithm(config)
+    batch_index.value = eng.run_epoch(batch_index.value, beat_order=beat_order)

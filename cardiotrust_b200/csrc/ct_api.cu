@@ -1,0 +1,777 @@
+// C ABI and host-side epoch driver.
+//
+// ct_run_epoch mirrors run_epoch (src/core/algorithm.rs:124-281): reset the
+// derivatives, visit the beats in order, per beat reset the estimations and
+// run prediction -> residuals -> derivation -> step metrics for all steps,
+// then (per batch or per epoch) average delays -> batch derivatives ->
+// APParameters::update -> batch metrics. The per-step work of one beat runs
+// as five kernels over all steps (forward, H x, H^T r, derivation, metrics)
+// instead of T x 15 small launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ct_internal.cuh"
+
+using ct::DeviceScenario;
+using ct::kGainCols;
+using ct::kOffsets;
+
+struct ct_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int num_sms = 0;
+};
+
+struct PhaseEvents {
+  int phase;
+  cudaEvent_t start, stop;
+};
+
+struct ct_scn {
+  ct_ctx* ctx = nullptr;
+  ct_algorithm algo{};
+  DeviceScenario d{};
+  int64_t adam_step = 1;  // Derivatives.step, derivation.rs:100
+  uint64_t rng = 0x9e3779b97f4a7c15ull;
+  std::vector<void*> allocations;
+  std::vector<int32_t> nbr_host;  // neighbour table, for validating delay writes
+  // launch accounting and optional per-phase CUDA-event timing
+  int64_t launches = 0;
+  bool profiling = false;
+  double phase_ms[CT_PHASE_COUNT] = {};
+  int64_t phase_launches[CT_PHASE_COUNT] = {};
+  std::vector<PhaseEvents> pending;
+  std::vector<cudaEvent_t> event_pool;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return status;
+}
+
+int cuda_fail(cudaError_t err, const char* what) {
+  return fail(err == cudaErrorMemoryAllocation ? CT_ERR_OUT_OF_MEMORY : CT_ERR_CUDA, "%s: %s", what,
+              cudaGetErrorString(err));
+}
+
+#define CT_CUDA(call, what)                    \
+  do {                                         \
+    cudaError_t err__ = (call);                \
+    if (err__ != cudaSuccess) return cuda_fail(err__, what); \
+  } while (0)
+
+cudaEvent_t take_event(ct_scn* s) {
+  if (!s->event_pool.empty()) {
+    cudaEvent_t e = s->event_pool.back();
+    s->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  return e;
+}
+
+// Runs one phase: counts its kernel launches and, when profiling, brackets it
+// with CUDA events on the context stream (the stream every kernel uses).
+template <typename F>
+cudaError_t run_phase(ct_scn* s, int phase, int kernels, F&& body) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (s->profiling) {
+    e0 = take_event(s);
+    e1 = take_event(s);
+    if (e0) cudaEventRecord(e0, s->ctx->stream);
+  }
+  cudaError_t err = body();
+  s->launches += kernels;
+  if (s->profiling && e0 && e1) {
+    cudaEventRecord(e1, s->ctx->stream);
+    s->pending.push_back({phase, e0, e1});
+    s->phase_launches[phase] += kernels;
+  }
+  return err;
+}
+
+template <typename T>
+int alloc(ct_scn* s, T** p, int64_t count) {
+  void* ptr = nullptr;
+  const size_t bytes = sizeof(T) * (size_t)(count > 0 ? count : 1);
+  cudaError_t err = cudaMalloc(&ptr, bytes);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc");
+  s->allocations.push_back(ptr);
+  *p = static_cast<T*>(ptr);
+  return CT_OK;
+}
+
+int upload(ct_scn* s, void* dst, const void* src, size_t bytes) {
+  CT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->ctx->stream), "upload");
+  return CT_OK;
+}
+
+int check_algo(const ct_algorithm* a) {
+  if (!a) return fail(CT_ERR_INVALID_ARGUMENT, "algorithm is NULL");
+  if (a->optimizer != CT_OPT_SGD && a->optimizer != CT_OPT_ADAM)
+    return fail(CT_ERR_INVALID_ARGUMENT, "unknown optimizer %d", a->optimizer);
+  if (a->ap_derivative != CT_AP_SIMPLE && a->ap_derivative != CT_AP_TEXTBOOK)
+    return fail(CT_ERR_INVALID_ARGUMENT, "unknown ap_derivative %d", a->ap_derivative);
+  if (a->batch_size < 0) return fail(CT_ERR_INVALID_ARGUMENT, "negative batch_size");
+  return CT_OK;
+}
+
+// Shuffle of the beat indices when the caller passes no order (the reference
+// shuffles with an unseeded generator, algorithm.rs:139-141).
+void seeded_shuffle(ct_scn* s, std::vector<int32_t>& order) {
+  for (size_t i = order.size(); i > 1; --i) {
+    s->rng ^= s->rng << 13;
+    s->rng ^= s->rng >> 7;
+    s->rng ^= s->rng << 17;
+    const size_t j = (size_t)(s->rng % i);
+    std::swap(order[i - 1], order[j]);
+  }
+}
+
+int run_beat(ct_scn* s, int64_t beat) {
+  DeviceScenario& d = s->d;
+  const ct_algorithm& a = s->algo;
+  cudaStream_t st = s->ctx->stream;
+  CT_CUDA(run_phase(s, CT_PHASE_FORWARD, 1,
+                    [&] { return ct::launch_forward(d, a.maximum_regularization_threshold, st); }),
+          "forward kernel");
+  CT_CUDA(run_phase(s, CT_PHASE_MEASURE, 3, [&] { return ct::launch_measure(d, beat, true, st); }),
+          "measurement kernel");
+  CT_CUDA(run_phase(s, CT_PHASE_MAP_RESIDUALS, 1, [&] { return ct::launch_map_residuals(d, beat, st); }),
+          "mapped-residual kernel");
+  if (!a.freeze_gains || !a.freeze_delays) {
+    ct::DeriveScalars ds;
+    ds.mse_scaling = 1.0f / (float)d.M * a.mse_strength;
+    ds.reg_scaling = a.maximum_regularization_strength;
+    ds.threshold = a.maximum_regularization_threshold;
+    ds.diffreg = a.difference_regularization_strength;
+    ds.freeze_gains = a.freeze_gains;
+    ds.freeze_delays = a.freeze_delays;
+    ds.ap_derivative = a.ap_derivative;
+    CT_CUDA(run_phase(s, CT_PHASE_DERIVE, 1, [&] { return ct::launch_derive(d, ds, st); }), "derivation kernel");
+  }
+  CT_CUDA(run_phase(s, CT_PHASE_STEP_METRICS, 1,
+                    [&] { return ct::launch_step_metrics(d, a.maximum_regularization_strength, st); }),
+          "step metrics kernel");
+  return CT_OK;
+}
+
+int derivatives_reset(ct_scn* s) {
+  DeviceScenario& d = s->d;
+  cudaStream_t st = s->ctx->stream;
+  CT_CUDA(cudaMemsetAsync(d.dG, 0, sizeof(float) * d.S * kGainCols, st), "reset");
+  CT_CUDA(cudaMemsetAsync(d.dC, 0, sizeof(float) * d.V * kOffsets, st), "reset");
+  CT_CUDA(cudaMemsetAsync(d.fir, 0, sizeof(float) * d.V * kGainCols, st), "reset");
+  CT_CUDA(cudaMemsetAsync(d.iir, 0, sizeof(float) * d.V * kGainCols, st), "reset");
+  CT_CUDA(cudaMemsetAsync(d.mreg_sum, 0, sizeof(float), st), "reset");
+  return CT_OK;
+}
+
+// calculate_average_delays -> calculate_batch_derivatives -> update -> calculate_batch
+int batch_end(ct_scn* s, int64_t n_beats, int64_t* batch_index) {
+  DeviceScenario& d = s->d;
+  const ct_algorithm& a = s->algo;
+  cudaStream_t st = s->ctx->stream;
+  if (*batch_index < 0 || *batch_index >= d.NB)
+    return fail(CT_ERR_BATCH_INDEX, "batch index %lld outside the %lld batch-wise metric slots",
+                (long long)*batch_index, (long long)d.NB);
+  const bool smooth = !a.freeze_delays && std::fabs(a.smoothness_regularization_strength) > 1.1920929e-7f;
+  const int kernels = 1 + (smooth ? 1 : 0) + (a.freeze_gains ? 0 : 1) + (a.freeze_delays ? 0 : 4) + 1;
+  cudaError_t err = run_phase(s, CT_PHASE_UPDATE, kernels, [&]() -> cudaError_t {
+  cudaError_t e = ct::launch_average_delays(d, st);
+  if (e != cudaSuccess) return e;
+  if (smooth) {
+    e = ct::launch_smoothness(d, a.smoothness_regularization_strength, st);
+    if (e != cudaSuccess) return e;
+  }
+  const int64_t bs = (a.batch_size == 0) ? d.T * n_beats : d.T * a.batch_size;
+  ct::UpdateScalars u;
+  u.optimizer = a.optimizer;
+  u.freeze_gains = a.freeze_gains;
+  u.freeze_delays = a.freeze_delays;
+  u.lr_over_bs = a.learning_rate / (float)bs;
+  // update.rs:140-141: 1 - beta^step with f32 powf
+  u.bias1 = 1.0f - powf(0.9f, (float)s->adam_step);
+  u.bias2 = 1.0f - powf(0.999f, (float)s->adam_step);
+  e = ct::launch_update(d, u, st);
+  if (e != cudaSuccess) return e;
+  if (!a.freeze_delays) {
+    e = ct::launch_min_delay(d, st);
+    if (e != cudaSuccess) return e;
+  }
+  return ct::launch_batch_metrics(d, *batch_index, st);
+  });
+  if (err != cudaSuccess) return cuda_fail(err, "update kernels");
+  s->adam_step += 1;
+  *batch_index += 1;
+  return CT_OK;
+}
+
+int validate_and_build_nbr(const ct_scenario_desc* desc, std::vector<int32_t>& nbr) {
+  const int64_t S = desc->num_states, V = S / 3;
+  nbr.assign((size_t)(V * kOffsets), -1);
+  const int32_t* osi = desc->output_state_indices;
+  for (int64_t v = 0; v < V; ++v) {
+    for (int n = 0; n < kOffsets; ++n) {
+      const int32_t first = osi[(3 * v) * kGainCols + 3 * n];
+      int32_t nb = -1;
+      if (first >= 0) {
+        if (first % 3 != 0 || first / 3 >= V)
+          return fail(CT_ERR_INVALID_INDEX, "output_state_indices[%lld,%d] = %d is not a voxel's first state",
+                      (long long)(3 * v), 3 * n, first);
+        nb = first / 3;
+      }
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          const int32_t got = osi[(3 * v + a) * kGainCols + 3 * n + b];
+          const int32_t want = nb < 0 ? -1 : 3 * nb + b;
+          if ((got < 0 ? -1 : got) != want)
+            return fail(CT_ERR_INVALID_INDEX,
+                        "output_state_indices[%lld,%d] = %d breaks the (voxel, offset, component) structure",
+                        (long long)(3 * v + a), 3 * n + b, got);
+        }
+      nbr[(size_t)(v * kOffsets + n)] = nb;
+      if (nb >= 0 && desc->delays[v * kOffsets + n] < 1)
+        return fail(CT_ERR_INVALID_ARGUMENT, "delay of connected pair (%lld,%d) is %d; delays must be >= 1",
+                    (long long)v, n, desc->delays[v * kOffsets + n]);
+    }
+  }
+  return CT_OK;
+}
+
+void free_scenario(ct_scn* s) {
+  for (void* p : s->allocations) cudaFree(p);
+  s->allocations.clear();
+  for (auto& pe : s->pending) {
+    cudaEventDestroy(pe.start);
+    cudaEventDestroy(pe.stop);
+  }
+  s->pending.clear();
+  for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
+  s->event_pool.clear();
+}
+
+int field_bytes(const ct_scn* s, int field, size_t* nbytes) {
+  const DeviceScenario& d = s->d;
+  const size_t f = sizeof(float);
+  switch (field) {
+    case CT_FIELD_GAINS:
+    case CT_FIELD_AP_OUTPUTS_NOW:
+    case CT_FIELD_AP_OUTPUTS_LAST:
+    case CT_FIELD_GRAD_GAINS:
+    case CT_FIELD_COEFS_FIR:
+    case CT_FIELD_COEFS_IIR:
+    case CT_FIELD_GAINS_FIRST_MOMENT:
+    case CT_FIELD_GAINS_SECOND_MOMENT: *nbytes = f * d.S * kGainCols; return CT_OK;
+    case CT_FIELD_COEFS:
+    case CT_FIELD_GRAD_COEFS:
+    case CT_FIELD_COEFS_FIRST_MOMENT:
+    case CT_FIELD_COEFS_SECOND_MOMENT: *nbytes = f * d.V * kOffsets; return CT_OK;
+    case CT_FIELD_DELAYS: *nbytes = sizeof(int32_t) * d.V * kOffsets; return CT_OK;
+    case CT_FIELD_MEASUREMENTS_ACTUAL:
+    case CT_FIELD_MEASUREMENTS: *nbytes = f * d.B * d.T * d.M; return CT_OK;
+    case CT_FIELD_SYSTEM_STATES:
+    case CT_FIELD_MAPPED_RESIDUALS_HISTORY: *nbytes = f * d.T * d.S; return CT_OK;
+    case CT_FIELD_RESIDUALS: *nbytes = f * d.M; return CT_OK;
+    case CT_FIELD_AVERAGE_DELAYS: *nbytes = f * d.V; return CT_OK;
+    case CT_FIELD_MAPPED_RESIDUALS:
+    case CT_FIELD_MAXIMUM_REGULARIZATION: *nbytes = f * d.S; return CT_OK;
+    case CT_FIELD_MAXIMUM_REGULARIZATION_SUM: *nbytes = f; return CT_OK;
+    case CT_FIELD_ADAM_STEP: *nbytes = sizeof(int64_t); return CT_OK;
+    case CT_FIELD_LOSS:
+    case CT_FIELD_LOSS_MSE:
+    case CT_FIELD_LOSS_MAXIMUM_REGULARIZATION: *nbytes = f * d.T; return CT_OK;
+    case CT_FIELD_LOSS_BATCH:
+    case CT_FIELD_LOSS_MSE_BATCH:
+    case CT_FIELD_LOSS_MAXIMUM_REGULARIZATION_BATCH: *nbytes = f * d.NB; return CT_OK;
+    default: return fail(CT_ERR_INVALID_ARGUMENT, "unknown field %d", field);
+  }
+}
+
+int copy_down(ct_scn* s, void* dst, const void* src, size_t bytes) {
+  CT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->ctx->stream), "read field");
+  CT_CUDA(cudaStreamSynchronize(s->ctx->stream), "read field");
+  return CT_OK;
+}
+
+// [V,78] device -> [S,78] host (row component replicated)
+int copy_down_expanded(ct_scn* s, float* dst, const float* src) {
+  const int64_t V = s->d.V;
+  std::vector<float> tmp((size_t)(V * kGainCols));
+  int rc = copy_down(s, tmp.data(), src, sizeof(float) * tmp.size());
+  if (rc) return rc;
+  for (int64_t v = 0; v < V; ++v)
+    for (int a = 0; a < 3; ++a)
+      std::memcpy(dst + (3 * v + a) * kGainCols, tmp.data() + v * kGainCols, sizeof(float) * kGainCols);
+  return CT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ct_version(void) { return CT_ABI_VERSION; }
+
+const char* ct_status_string(int status) {
+  switch (status) {
+    case CT_OK: return "ok";
+    case CT_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case CT_ERR_CUDA: return "CUDA error";
+    case CT_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case CT_ERR_TIMEOUT: return "device-side wait timed out";
+    case CT_ERR_INVALID_INDEX: return "output_state_indices lack the voxel/neighbour structure";
+    case CT_ERR_NOT_SUPPORTED: return "not supported";
+    case CT_ERR_BATCH_INDEX: return "batch index outside the metric arrays";
+    default: return "unknown status";
+  }
+}
+
+int ct_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return CT_ERR_INVALID_ARGUMENT;
+  std::snprintf(buf, len, "%s", g_last_error.c_str());
+  return CT_OK;
+}
+
+int ct_ctx_create(int device, void* stream, ct_ctx** out) {
+  if (!out) return fail(CT_ERR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  int count = 0;
+  CT_CUDA(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+  if (device < 0 || device >= count) return fail(CT_ERR_INVALID_ARGUMENT, "device %d of %d", device, count);
+  CT_CUDA(cudaSetDevice(device), "cudaSetDevice");
+  ct_ctx* c = new ct_ctx;
+  c->device = device;
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (stream) {
+    c->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    cudaError_t err = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) {
+      delete c;
+      return cuda_fail(err, "cudaStreamCreate");
+    }
+    c->own_stream = true;
+  }
+  *out = c;
+  return CT_OK;
+}
+
+int ct_ctx_destroy(ct_ctx* ctx) {
+  if (!ctx) return CT_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return CT_OK;
+}
+
+int ct_ctx_stream(ct_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *stream = ctx->stream;
+  return CT_OK;
+}
+
+int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algorithm* algo, ct_scn** out) {
+  if (!ctx || !desc || !out) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  int rc = check_algo(algo);
+  if (rc) return rc;
+  const int64_t S = desc->num_states, M = desc->num_sensors, T = desc->num_steps, B = desc->num_beats;
+  if (S <= 0 || S % 3 != 0) return fail(CT_ERR_INVALID_ARGUMENT, "num_states %lld must be a positive multiple of 3", (long long)S);
+  if (M <= 0 || T <= 0 || B <= 0) return fail(CT_ERR_INVALID_ARGUMENT, "num_sensors, num_steps and num_beats must be positive");
+  if (desc->num_batch_slots <= 0) return fail(CT_ERR_INVALID_ARGUMENT, "num_batch_slots must be positive");
+  if (!desc->gains || !desc->output_state_indices || !desc->coefs || !desc->delays || !desc->initial_delays ||
+      !desc->measurement_matrix || !desc->control_matrix || !desc->control_function)
+    return fail(CT_ERR_INVALID_ARGUMENT, "a required array pointer is NULL");
+  std::vector<int32_t> nbr;
+  rc = validate_and_build_nbr(desc, nbr);
+  if (rc) return rc;
+  CT_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+
+  ct_scn* s = new ct_scn;
+  s->ctx = ctx;
+  s->algo = *algo;
+  s->nbr_host = nbr;
+  DeviceScenario& d = s->d;
+  d.S = S;
+  d.V = S / 3;
+  d.M = M;
+  d.T = T;
+  d.B = B;
+  d.NB = desc->num_batch_slots;
+  d.fwd_grid = ct::forward_grid_size(d.V, ctx->device);
+  {
+    const int64_t tiles = ((M + 63) / 64) * ((T + 63) / 64);
+    int64_t ks = (2 * ctx->num_sms + tiles - 1) / tiles;
+    ks = std::min<int64_t>(ks, std::max<int64_t>(1, S / 256));
+    d.ksplit = (int)std::max<int64_t>(1, std::min<int64_t>(ks, 64));
+  }
+  const int64_t V = d.V, mpad = ((M + 63) / 64) * 64;
+#define ALLOC(ptr, n)                    \
+  do {                                   \
+    int r__ = alloc(s, &(ptr), (n));     \
+    if (r__) {                           \
+      free_scenario(s);                  \
+      delete s;                          \
+      return r__;                        \
+    }                                    \
+  } while (0)
+  ALLOC(d.gains, S * kGainCols);
+  ALLOC(d.nbr, V * kOffsets);
+  ALLOC(d.coefs, V * kOffsets);
+  ALLOC(d.delays, V * kOffsets);
+  ALLOC(d.init_delays, V * kOffsets);
+  ALLOC(d.H, B * M * S);
+  ALLOC(d.ctrl, S);
+  ALLOC(d.u, T);
+  ALLOC(d.meas, B * T * M);
+  ALLOC(d.X, T * S);
+  ALLOC(d.Y, B * T * M);
+  ALLOC(d.R, T * M);
+  ALLOC(d.MR, T * S);
+  ALLOC(d.ap, V * kGainCols);
+  ALLOC(d.ap_last, V * kGainCols);
+  ALLOC(d.avg_delays, V);
+  ALLOC(d.dG, S * kGainCols);
+  ALLOC(d.dC, V * kOffsets);
+  ALLOC(d.fir, V * kGainCols);
+  ALLOC(d.iir, V * kGainCols);
+  ALLOC(d.mG1, S * kGainCols);
+  ALLOC(d.mG2, S * kGainCols);
+  ALLOC(d.mC1, V * kOffsets);
+  ALLOC(d.mC2, V * kOffsets);
+  ALLOC(d.mreg_sum, 1);
+  ALLOC(d.loss, T);
+  ALLOC(d.loss_mse, T);
+  ALLOC(d.loss_mr, T);
+  ALLOC(d.loss_b, d.NB);
+  ALLOC(d.loss_mse_b, d.NB);
+  ALLOC(d.loss_mr_b, d.NB);
+  ALLOC(d.stepsum_part, T * d.fwd_grid);
+  ALLOC(d.gemm_part, (int64_t)d.ksplit * T * mpad);
+  ALLOC(d.dmin, 1);
+  ALLOC(d.status, 1);
+  ALLOC(d.barrier, 1);
+#undef ALLOC
+  cudaStream_t st = ctx->stream;
+  int r = CT_OK;
+  r = r ? r : upload(s, d.gains, desc->gains, sizeof(float) * S * kGainCols);
+  r = r ? r : upload(s, d.nbr, nbr.data(), sizeof(int32_t) * V * kOffsets);
+  r = r ? r : upload(s, d.coefs, desc->coefs, sizeof(float) * V * kOffsets);
+  r = r ? r : upload(s, d.delays, desc->delays, sizeof(int32_t) * V * kOffsets);
+  r = r ? r : upload(s, d.init_delays, desc->initial_delays, sizeof(float) * V * kOffsets);
+  r = r ? r : upload(s, d.H, desc->measurement_matrix, sizeof(float) * B * M * S);
+  r = r ? r : upload(s, d.ctrl, desc->control_matrix, sizeof(float) * S);
+  r = r ? r : upload(s, d.u, desc->control_function, sizeof(float) * T);
+  if (!r && desc->measurements) r = upload(s, d.meas, desc->measurements, sizeof(float) * B * T * M);
+  if (!r && !desc->measurements) {
+    cudaError_t e = cudaMemsetAsync(d.meas, 0, sizeof(float) * B * T * M, st);
+    if (e != cudaSuccess) r = cuda_fail(e, "memset");
+  }
+  auto zero = [&](void* p, size_t bytes) {
+    if (r) return;
+    cudaError_t e = cudaMemsetAsync(p, 0, bytes, st);
+    if (e != cudaSuccess) r = cuda_fail(e, "memset");
+  };
+  zero(d.X, sizeof(float) * T * S);
+  zero(d.Y, sizeof(float) * B * T * M);
+  zero(d.R, sizeof(float) * T * M);
+  zero(d.MR, sizeof(float) * T * S);
+  zero(d.ap, sizeof(float) * V * kGainCols);
+  zero(d.ap_last, sizeof(float) * V * kGainCols);
+  zero(d.dG, sizeof(float) * S * kGainCols);
+  zero(d.dC, sizeof(float) * V * kOffsets);
+  zero(d.fir, sizeof(float) * V * kGainCols);
+  zero(d.iir, sizeof(float) * V * kGainCols);
+  zero(d.mG1, sizeof(float) * S * kGainCols);
+  zero(d.mG2, sizeof(float) * S * kGainCols);
+  zero(d.mC1, sizeof(float) * V * kOffsets);
+  zero(d.mC2, sizeof(float) * V * kOffsets);
+  zero(d.mreg_sum, sizeof(float));
+  zero(d.loss, sizeof(float) * T);
+  zero(d.loss_mse, sizeof(float) * T);
+  zero(d.loss_mr, sizeof(float) * T);
+  zero(d.loss_b, sizeof(float) * d.NB);
+  zero(d.loss_mse_b, sizeof(float) * d.NB);
+  zero(d.loss_mr_b, sizeof(float) * d.NB);
+  zero(d.status, sizeof(int32_t));
+  zero(d.barrier, sizeof(ct::GridBarrier));
+  std::vector<float> nan_v((size_t)V, std::nanf(""));
+  r = r ? r : upload(s, d.avg_delays, nan_v.data(), sizeof(float) * V);
+  if (!r) {
+    cudaError_t e = ct::launch_min_delay(d, st);
+    if (e != cudaSuccess) r = cuda_fail(e, "min delay kernel");
+  }
+  if (!r) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) r = cuda_fail(e, "scenario upload");
+  }
+  if (r) {
+    free_scenario(s);
+    delete s;
+    return r;
+  }
+  *out = s;
+  return CT_OK;
+}
+
+int ct_scenario_destroy(ct_scn* scn) {
+  if (!scn) return CT_OK;
+  cudaSetDevice(scn->ctx->device);
+  cudaStreamSynchronize(scn->ctx->stream);
+  free_scenario(scn);
+  delete scn;
+  return CT_OK;
+}
+
+int ct_scenario_dims(ct_scn* scn, int64_t* S, int64_t* M, int64_t* T, int64_t* B) {
+  if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
+  if (S) *S = scn->d.S;
+  if (M) *M = scn->d.M;
+  if (T) *T = scn->d.T;
+  if (B) *B = scn->d.B;
+  return CT_OK;
+}
+
+int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, int grad_mode, int precision) {
+  if (!scn || !batch_index) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (grad_mode != CT_GRAD_REFERENCE) return fail(CT_ERR_NOT_SUPPORTED, "gradient mode %d", grad_mode);
+  if (precision != CT_PREC_FP32) return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  DeviceScenario& d = scn->d;
+  const ct_algorithm& a = scn->algo;
+  std::vector<int32_t> order((size_t)d.B);
+  if (beat_order) {
+    for (int64_t i = 0; i < d.B; ++i) {
+      if (beat_order[i] < 0 || beat_order[i] >= d.B)
+        return fail(CT_ERR_INVALID_ARGUMENT, "beat_order[%lld] = %d out of range", (long long)i, beat_order[i]);
+      order[(size_t)i] = beat_order[i];
+    }
+  } else {
+    for (int64_t i = 0; i < d.B; ++i) order[(size_t)i] = (int32_t)i;
+    seeded_shuffle(scn, order);
+  }
+  int rc = derivatives_reset(scn);
+  if (rc) return rc;
+  int64_t batch = 0;
+  const bool batched = a.batch_size != 0;
+  for (int32_t beat : order) {
+    rc = run_beat(scn, beat);
+    if (rc) return rc;
+    if (batched) {
+      batch += 1;
+      if (batch == a.batch_size) {
+        rc = batch_end(scn, batch, batch_index);
+        if (rc) return rc;
+        rc = derivatives_reset(scn);
+        if (rc) return rc;
+        batch = 0;
+      }
+    }
+  }
+  if (batched) return batch > 0 ? batch_end(scn, batch, batch_index) : CT_OK;
+  return batch_end(scn, d.B, batch_index);
+}
+
+int ct_simulate(ct_scn* scn, float* measurements_out, float* states_out) {
+  if (!scn || !measurements_out) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  DeviceScenario& d = scn->d;
+  cudaStream_t st = scn->ctx->stream;
+  for (int64_t beat = 0; beat < d.B; ++beat) {
+    CT_CUDA(run_phase(scn, CT_PHASE_FORWARD, 1,
+                      [&] { return ct::launch_forward(d, scn->algo.maximum_regularization_threshold, st); }),
+            "forward kernel");
+    CT_CUDA(run_phase(scn, CT_PHASE_MEASURE, 2, [&] { return ct::launch_measure(d, beat, false, st); }),
+            "measurement kernel");
+  }
+  int rc = ct_sync(scn);
+  if (rc) return rc;
+  rc = copy_down(scn, measurements_out, d.Y, sizeof(float) * d.B * d.T * d.M);
+  if (rc) return rc;
+  if (states_out) rc = copy_down(scn, states_out, d.X, sizeof(float) * d.T * d.S);
+  return rc;
+}
+
+int ct_set_algorithm(ct_scn* scn, const ct_algorithm* algo) {
+  if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
+  int rc = check_algo(algo);
+  if (rc) return rc;
+  scn->algo = *algo;
+  return CT_OK;
+}
+
+int ct_set_freeze(ct_scn* scn, int freeze_gains, int freeze_delays) {
+  if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
+  scn->algo.freeze_gains = freeze_gains != 0;
+  scn->algo.freeze_delays = freeze_delays != 0;
+  return CT_OK;
+}
+
+int ct_set_learning_rate(ct_scn* scn, float learning_rate) {
+  if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
+  scn->algo.learning_rate = learning_rate;
+  return CT_OK;
+}
+
+int ct_field_size(ct_scn* scn, int field, size_t* nbytes) {
+  if (!scn || !nbytes) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  return field_bytes(scn, field, nbytes);
+}
+
+int ct_read_field(ct_scn* scn, int field, void* dst, size_t nbytes) {
+  if (!scn || !dst) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  size_t want = 0;
+  int rc = field_bytes(scn, field, &want);
+  if (rc) return rc;
+  if (want != nbytes) return fail(CT_ERR_INVALID_ARGUMENT, "field %d has %zu bytes, got %zu", field, want, nbytes);
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  DeviceScenario& d = scn->d;
+  float* out = static_cast<float*>(dst);
+  switch (field) {
+    case CT_FIELD_GAINS: return copy_down(scn, dst, d.gains, nbytes);
+    case CT_FIELD_COEFS: return copy_down(scn, dst, d.coefs, nbytes);
+    case CT_FIELD_DELAYS: return copy_down(scn, dst, d.delays, nbytes);
+    case CT_FIELD_MEASUREMENTS_ACTUAL: return copy_down(scn, dst, d.meas, nbytes);
+    case CT_FIELD_SYSTEM_STATES: return copy_down(scn, dst, d.X, nbytes);
+    case CT_FIELD_MEASUREMENTS: return copy_down(scn, dst, d.Y, nbytes);
+    case CT_FIELD_RESIDUALS: return copy_down(scn, dst, d.R + (d.T - 1) * d.M, nbytes);
+    case CT_FIELD_AP_OUTPUTS_NOW: return copy_down_expanded(scn, out, d.ap);
+    case CT_FIELD_AP_OUTPUTS_LAST: return copy_down_expanded(scn, out, d.ap_last);
+    case CT_FIELD_AVERAGE_DELAYS: return copy_down(scn, dst, d.avg_delays, nbytes);
+    case CT_FIELD_GRAD_GAINS: return copy_down(scn, dst, d.dG, nbytes);
+    case CT_FIELD_GRAD_COEFS: return copy_down(scn, dst, d.dC, nbytes);
+    case CT_FIELD_COEFS_FIR: return copy_down_expanded(scn, out, d.fir);
+    case CT_FIELD_COEFS_IIR: return copy_down_expanded(scn, out, d.iir);
+    case CT_FIELD_MAPPED_RESIDUALS: return copy_down(scn, dst, d.MR + (d.T - 1) * d.S, nbytes);
+    case CT_FIELD_MAXIMUM_REGULARIZATION: {
+      // derived from the last step's states into a temporary device buffer (read-back path only)
+      float* tmp = nullptr;
+      CT_CUDA(cudaMallocAsync((void**)&tmp, nbytes, scn->ctx->stream), "cudaMallocAsync");
+      cudaError_t e = ct::launch_last_max_reg(d, scn->algo.maximum_regularization_threshold, tmp, scn->ctx->stream);
+      int r2 = e == cudaSuccess ? copy_down(scn, dst, tmp, nbytes) : cuda_fail(e, "max reg kernel");
+      cudaFreeAsync(tmp, scn->ctx->stream);
+      return r2;
+    }
+    case CT_FIELD_MAXIMUM_REGULARIZATION_SUM: return copy_down(scn, dst, d.mreg_sum, nbytes);
+    case CT_FIELD_ADAM_STEP: std::memcpy(dst, &scn->adam_step, sizeof(int64_t)); return CT_OK;
+    case CT_FIELD_GAINS_FIRST_MOMENT: return copy_down(scn, dst, d.mG1, nbytes);
+    case CT_FIELD_GAINS_SECOND_MOMENT: return copy_down(scn, dst, d.mG2, nbytes);
+    case CT_FIELD_COEFS_FIRST_MOMENT: return copy_down(scn, dst, d.mC1, nbytes);
+    case CT_FIELD_COEFS_SECOND_MOMENT: return copy_down(scn, dst, d.mC2, nbytes);
+    case CT_FIELD_MAPPED_RESIDUALS_HISTORY: return copy_down(scn, dst, d.MR, nbytes);
+    case CT_FIELD_LOSS: return copy_down(scn, dst, d.loss, nbytes);
+    case CT_FIELD_LOSS_MSE: return copy_down(scn, dst, d.loss_mse, nbytes);
+    case CT_FIELD_LOSS_MAXIMUM_REGULARIZATION: return copy_down(scn, dst, d.loss_mr, nbytes);
+    case CT_FIELD_LOSS_BATCH: return copy_down(scn, dst, d.loss_b, nbytes);
+    case CT_FIELD_LOSS_MSE_BATCH: return copy_down(scn, dst, d.loss_mse_b, nbytes);
+    case CT_FIELD_LOSS_MAXIMUM_REGULARIZATION_BATCH: return copy_down(scn, dst, d.loss_mr_b, nbytes);
+    default: return fail(CT_ERR_INVALID_ARGUMENT, "unknown field %d", field);
+  }
+}
+
+int ct_write_field(ct_scn* scn, int field, const void* src, size_t nbytes) {
+  if (!scn || !src) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  size_t want = 0;
+  int rc = field_bytes(scn, field, &want);
+  if (rc) return rc;
+  if (want != nbytes) return fail(CT_ERR_INVALID_ARGUMENT, "field %d has %zu bytes, got %zu", field, want, nbytes);
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  DeviceScenario& d = scn->d;
+  void* dst = nullptr;
+  switch (field) {
+    case CT_FIELD_GAINS: dst = d.gains; break;
+    case CT_FIELD_COEFS: dst = d.coefs; break;
+    case CT_FIELD_DELAYS: {
+      const int32_t* del = static_cast<const int32_t*>(src);
+      const std::vector<int32_t>& nbr = scn->nbr_host;
+      for (size_t i = 0; i < nbr.size(); ++i)
+        if (nbr[i] >= 0 && del[i] < 1)
+          return fail(CT_ERR_INVALID_ARGUMENT, "delay %zu of a connected pair is %d; delays must be >= 1", i, del[i]);
+      dst = d.delays;
+      break;
+    }
+    case CT_FIELD_MEASUREMENTS_ACTUAL: dst = d.meas; break;
+    default: return fail(CT_ERR_INVALID_ARGUMENT, "field %d is read-only", field);
+  }
+  CT_CUDA(cudaMemcpyAsync(dst, src, nbytes, cudaMemcpyHostToDevice, scn->ctx->stream), "write field");
+  if (field == CT_FIELD_DELAYS) CT_CUDA(ct::launch_min_delay(d, scn->ctx->stream), "min delay kernel");
+  CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "write field");
+  return CT_OK;
+}
+
+int ct_sync(ct_scn* scn) {
+  if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "cudaStreamSynchronize");
+  int32_t status = 0;
+  CT_CUDA(cudaMemcpy(&status, scn->d.status, sizeof(int32_t), cudaMemcpyDeviceToHost), "read status");
+  if (status != 0) {
+    cudaMemset(scn->d.status, 0, sizeof(int32_t));
+    return fail(status, "device-side failure: %s", ct_status_string(status));
+  }
+  return CT_OK;
+}
+
+int ct_kernel_launches(ct_scn* scn, int64_t* launches) {
+  if (!scn || !launches) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *launches = scn->launches;
+  return CT_OK;
+}
+
+int ct_set_profiling(ct_scn* scn, int enable) {
+  if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "cudaStreamSynchronize");
+  for (auto& pe : scn->pending) {
+    scn->event_pool.push_back(pe.start);
+    scn->event_pool.push_back(pe.stop);
+  }
+  scn->pending.clear();
+  scn->profiling = enable != 0;
+  if (scn->profiling) {
+    for (int i = 0; i < CT_PHASE_COUNT; ++i) {
+      scn->phase_ms[i] = 0.0;
+      scn->phase_launches[i] = 0;
+    }
+  }
+  return CT_OK;
+}
+
+int ct_read_profile(ct_scn* scn, double* ms, int64_t* launches) {
+  if (!scn || !ms || !launches) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "cudaStreamSynchronize");
+  for (auto& pe : scn->pending) {
+    float t = 0.0f;
+    CT_CUDA(cudaEventElapsedTime(&t, pe.start, pe.stop), "cudaEventElapsedTime");
+    scn->phase_ms[pe.phase] += t;
+    scn->event_pool.push_back(pe.start);
+    scn->event_pool.push_back(pe.stop);
+  }
+  scn->pending.clear();
+  for (int i = 0; i < CT_PHASE_COUNT; ++i) {
+    ms[i] = scn->phase_ms[i];
+    launches[i] = scn->phase_launches[i];
+  }
+  return CT_OK;
+}
+
+}  // extern "C"

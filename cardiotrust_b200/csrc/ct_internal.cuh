@@ -1,0 +1,104 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/cardiotrust_cuda.h"
+
+namespace ct {
+
+constexpr int kOffsets = 26;   // neighbour offsets per voxel
+constexpr int kGainCols = 78;  // 26 offsets x 3 neighbour components
+constexpr int kMaxStepBlock = 8;  // steps advanced between grid barriers in the forward kernel
+
+// Spin limit of every device-side wait (~1 s of polling with a 64 ns back-off).
+constexpr long long kSpinLimit = 1ll << 24;
+
+// Device-side grid barrier state (generation counting).
+struct GridBarrier {
+  unsigned int count;
+  unsigned int generation;
+};
+
+// Everything of one scenario that lives on the device.
+struct DeviceScenario {
+  int64_t S, V, M, T, B, NB;
+  // model
+  float* gains;          // [S,78]
+  int32_t* nbr;          // [V,26] neighbour voxel, -1 = none (derived from output_state_indices)
+  float* coefs;          // [V,26]
+  int32_t* delays;       // [V,26]
+  float* init_delays;    // [V,26]
+  float* H;              // [B,M,S]
+  float* ctrl;           // [S]
+  float* u;              // [T]
+  float* meas;           // [B,T,M] actual measurements
+  // estimations
+  float* X;              // [T,S] states of the beat being processed
+  float* Y;              // [B,T,M] predicted measurements
+  float* R;              // [T,M] residuals of the beat being processed
+  float* MR;             // [T,S] mapped residuals of the beat being processed
+  float* ap;             // [V,78] all-pass state (deduplicated over the row component)
+  float* ap_last;        // [V,78] all-pass output of step T-2
+  float* avg_delays;     // [V]
+  // derivatives
+  float* dG;             // [S,78]
+  float* dC;             // [V,26]
+  float* fir;            // [V,78]
+  float* iir;            // [V,78]
+  float* mG1, *mG2;      // [S,78] Adam moments
+  float* mC1, *mC2;      // [V,26]
+  float* mreg_sum;       // [1] running maximum-regularisation sum
+  // metrics
+  float* loss, *loss_mse, *loss_mr;          // [T]
+  float* loss_b, *loss_mse_b, *loss_mr_b;    // [NB]
+  // scratch
+  float* stepsum_part;   // [T, fwd_grid] per-CTA partial max-regularisation sums
+  float* gemm_part;      // [ksplit, T, Mpad] split-K partials of H x
+  int fwd_grid;          // CTAs of the forward kernel
+  int ksplit;            // split-K factor of the H x product
+  int32_t* dmin;         // [1] smallest valid delay
+  int32_t* status;       // [1] device-side error code (0 = ok)
+  GridBarrier* barrier;  // [1]
+};
+
+// ---- launchers (all enqueue on `stream`, return cudaError_t of the launch)
+
+// Forward propagation of one beat: X[t,:] for t in [0,T).
+cudaError_t launch_forward(DeviceScenario& d, float threshold, cudaStream_t stream);
+int forward_grid_size(int64_t V, int device);
+
+// y = H[beat] x for all steps; Y[beat] = y, R = y - meas[beat], loss_mse[t].
+cudaError_t launch_measure(DeviceScenario& d, int64_t beat, bool with_residuals, cudaStream_t stream);
+// MR[t,:] = H[beat]^T R[t,:] for all steps.
+cudaError_t launch_map_residuals(DeviceScenario& d, int64_t beat, cudaStream_t stream);
+
+struct DeriveScalars {
+  float mse_scaling, reg_scaling, threshold, diffreg;
+  int freeze_gains, freeze_delays, ap_derivative;
+};
+// Per-(voxel, offset) sweep over the steps of one beat: dG, dC, fir, iir.
+cudaError_t launch_derive(DeviceScenario& d, const DeriveScalars& s, cudaStream_t stream);
+
+// Step metrics of one beat: loss_mr[t] (running), loss[t]; advances mreg_sum.
+cudaError_t launch_step_metrics(DeviceScenario& d, float reg_strength, cudaStream_t stream);
+// Batch metrics into slot `index`.
+cudaError_t launch_batch_metrics(DeviceScenario& d, int64_t index, cudaStream_t stream);
+
+cudaError_t launch_average_delays(DeviceScenario& d, cudaStream_t stream);
+cudaError_t launch_smoothness(DeviceScenario& d, float strength, cudaStream_t stream);
+
+struct UpdateScalars {
+  int optimizer, freeze_gains, freeze_delays;
+  float lr_over_bs, bias1, bias2;
+};
+cudaError_t launch_update(DeviceScenario& d, const UpdateScalars& s, cudaStream_t stream);
+cudaError_t launch_min_delay(DeviceScenario& d, cudaStream_t stream);
+
+// Expand the deduplicated [V,78] all-pass/fir/iir state into the reference [S,78] layout.
+cudaError_t launch_expand_rows(const float* src, float* dst, int64_t V, cudaStream_t stream);
+// Last-step maximum regularisation [S] from X[T-1].
+cudaError_t launch_last_max_reg(DeviceScenario& d, float threshold, float* out, cudaStream_t stream);
+
+}  // namespace ct

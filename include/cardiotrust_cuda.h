@@ -1,0 +1,194 @@
+/*
+ * cardiotrust_cuda.h — C ABI of the B200 estimation-epoch library.
+ *
+ * One scenario = one CardioTrust `Results` + `Model` + `Data` triple living in
+ * GPU memory. The entry points replace the reference crate's estimation epoch
+ * (paths relative to the crate root):
+ *
+ *   ct_run_epoch          <- run_epoch                    src/core/algorithm.rs:124-129
+ *                            EpochKernel::execute         src/core/algorithm/gpu/epoch.rs:96-117
+ *   ct_scenario_create    <- Results::to_gpu              src/core/scenario/results.rs:121-133
+ *                            EpochKernel::new             src/core/algorithm/gpu/epoch.rs:29-37
+ *   ct_read_field         <- Results::update_from_gpu     src/core/scenario/results.rs:136-147
+ *   ct_write_field        <- Results::to_gpu (per array)  src/core/scenario/results.rs:121-133
+ *   ct_set_freeze         <- EpochKernel::set_freeze_*    src/core/algorithm/gpu/epoch.rs:118-125
+ *   ct_set_learning_rate  <- Algorithm::learning_rate     src/core/config/algorithm.rs:35
+ *                            (mutated by the caller's schedule, src/core/scenario.rs:737-747)
+ *   ct_simulate           <- Simulation::run (forward)    src/core/data/simulation.rs:129-150
+ *   ct_ctx_create         <- GPU::new                     src/core/algorithm/gpu.rs:31-64
+ *
+ * Conventions: every function returns a status (CT_OK = 0, negative CT_ERR_*),
+ * never throws and never aborts. Host arrays passed in are copied; the caller
+ * keeps ownership. Handles are not thread-safe: use one scenario per host
+ * thread. All arrays are C-order, f32 unless stated, i32 for indices/delays.
+ * Shapes: S states, V = S/3 voxels, M sensor rows, T steps, B beats.
+ */
+#ifndef CARDIOTRUST_CUDA_H
+#define CARDIOTRUST_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CT_ABI_VERSION 1
+
+enum ct_status {
+  CT_OK = 0,
+  CT_ERR_INVALID_ARGUMENT = -1, /* null pointer, bad shape, bad enum */
+  CT_ERR_CUDA = -2,             /* a CUDA runtime call failed */
+  CT_ERR_OUT_OF_MEMORY = -3,    /* device allocation failed */
+  CT_ERR_TIMEOUT = -4,          /* a device-side wait hit its iteration limit */
+  CT_ERR_INVALID_INDEX = -5,    /* output_state_indices lack the voxel/neighbour structure */
+  CT_ERR_NOT_SUPPORTED = -6,    /* mode not available for this scenario */
+  CT_ERR_BATCH_INDEX = -7       /* batch-wise metric index outside the metric arrays */
+};
+
+/* Optimizer, src/core/algorithm/refinement.rs:8-12 */
+enum ct_optimizer { CT_OPT_SGD = 0, CT_OPT_ADAM = 1 };
+/* APDerivative, src/core/config/algorithm.rs:17-21 */
+enum ct_ap_derivative { CT_AP_SIMPLE = 0, CT_AP_TEXTBOOK = 1 };
+/* Gradient definition used by ct_run_epoch. */
+enum ct_grad_mode {
+  CT_GRAD_REFERENCE = 0 /* the reference's per-step derivation, derivation.rs:173-229 */
+};
+/* Arithmetic of the two measurement products (H x and H^T r). */
+enum ct_precision { CT_PREC_FP32 = 0 };
+
+/* The Algorithm fields the epoch reads, src/core/config/algorithm.rs:25-58. */
+typedef struct ct_algorithm {
+  int32_t optimizer;     /* ct_optimizer */
+  int32_t ap_derivative; /* ct_ap_derivative */
+  int32_t freeze_gains;
+  int32_t freeze_delays;
+  int64_t batch_size; /* 0 = one update per epoch */
+  float learning_rate;
+  float mse_strength;
+  float maximum_regularization_strength;
+  float maximum_regularization_threshold;
+  float difference_regularization_strength;
+  float smoothness_regularization_strength;
+} ct_algorithm;
+
+/* Host arrays describing one scenario (Model.functional_description + Data). */
+typedef struct ct_scenario_desc {
+  int64_t num_states;  /* S, multiple of 3 */
+  int64_t num_sensors; /* M */
+  int64_t num_steps;   /* T */
+  int64_t num_beats;   /* B */
+  int64_t num_batch_slots; /* length of the batch-wise metric arrays (epochs x batches) */
+  const float* gains;                  /* [S,78]  APParameters.gains, allpass.rs:30 */
+  const int32_t* output_state_indices; /* [S,78]  -1 = None, allpass.rs:31 / :146 */
+  const float* coefs;                  /* [V,26]  allpass.rs:32 */
+  const int32_t* delays;               /* [V,26]  allpass.rs:33 (usize, <= 1000 after roll_delays) */
+  const float* initial_delays;         /* [V,26]  allpass.rs:34 */
+  const float* measurement_matrix;     /* [B,M,S] measurement.rs:22 */
+  const float* control_matrix;         /* [S]     control.rs:23 */
+  const float* control_function;       /* [T]     control.rs:142 */
+  const float* measurements;           /* [B,T,M] data.simulation.measurements; may be NULL */
+} ct_scenario_desc;
+
+/* Arrays readable/writable with ct_read_field / ct_write_field. */
+enum ct_field {
+  /* model (read/write) */
+  CT_FIELD_GAINS = 0,           /* [S,78] f32 */
+  CT_FIELD_COEFS = 1,           /* [V,26] f32 */
+  CT_FIELD_DELAYS = 2,          /* [V,26] i32 */
+  CT_FIELD_MEASUREMENTS_ACTUAL = 3, /* [B,T,M] f32 */
+  /* estimations (read) */
+  CT_FIELD_SYSTEM_STATES = 10,  /* [T,S] f32 of the last beat run */
+  CT_FIELD_MEASUREMENTS = 11,   /* [B,T,M] f32 predicted */
+  CT_FIELD_RESIDUALS = 12,      /* [M] f32 last step */
+  CT_FIELD_AP_OUTPUTS_NOW = 13, /* [S,78] f32 */
+  CT_FIELD_AP_OUTPUTS_LAST = 14,/* [S,78] f32 */
+  CT_FIELD_AVERAGE_DELAYS = 15, /* [V] f32, NaN = None */
+  /* derivatives (read) */
+  CT_FIELD_GRAD_GAINS = 20,     /* [S,78] f32 */
+  CT_FIELD_GRAD_COEFS = 21,     /* [V,26] f32 */
+  CT_FIELD_COEFS_FIR = 22,      /* [S,78] f32 */
+  CT_FIELD_COEFS_IIR = 23,      /* [S,78] f32 */
+  CT_FIELD_MAPPED_RESIDUALS = 24,     /* [S] f32 last step */
+  CT_FIELD_MAXIMUM_REGULARIZATION = 25, /* [S] f32 last step */
+  CT_FIELD_MAXIMUM_REGULARIZATION_SUM = 26, /* [1] f32 */
+  CT_FIELD_ADAM_STEP = 27,      /* [1] i64, Derivatives.step */
+  CT_FIELD_GAINS_FIRST_MOMENT = 28,  /* [S,78] */
+  CT_FIELD_GAINS_SECOND_MOMENT = 29, /* [S,78] */
+  CT_FIELD_COEFS_FIRST_MOMENT = 30,  /* [V,26] */
+  CT_FIELD_COEFS_SECOND_MOMENT = 31, /* [V,26] */
+  CT_FIELD_MAPPED_RESIDUALS_HISTORY = 32, /* [T,S] f32 H^T r of every step of the last beat */
+  /* metrics (read) */
+  CT_FIELD_LOSS = 40,           /* [T] */
+  CT_FIELD_LOSS_MSE = 41,       /* [T] */
+  CT_FIELD_LOSS_MAXIMUM_REGULARIZATION = 42, /* [T] */
+  CT_FIELD_LOSS_BATCH = 43,     /* [num_batch_slots] */
+  CT_FIELD_LOSS_MSE_BATCH = 44,
+  CT_FIELD_LOSS_MAXIMUM_REGULARIZATION_BATCH = 45
+};
+
+typedef struct ct_ctx ct_ctx;
+typedef struct ct_scn ct_scn;
+
+int ct_version(void);
+const char* ct_status_string(int status);
+/* Last error message of the calling thread (empty if none). */
+int ct_last_error(char* buf, size_t len);
+
+/* Context = device + stream. stream == NULL creates a private non-blocking stream;
+ * otherwise the context issues all work on the given cudaStream_t. */
+int ct_ctx_create(int device, void* stream, ct_ctx** out);
+int ct_ctx_destroy(ct_ctx* ctx);
+int ct_ctx_stream(ct_ctx* ctx, void** stream);
+
+/* Copies the description to the device; Derivatives.step starts at 1 (derivation.rs:100). */
+int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algorithm* algo, ct_scn** out);
+int ct_scenario_destroy(ct_scn* scn);
+int ct_scenario_dims(ct_scn* scn, int64_t* S, int64_t* M, int64_t* T, int64_t* B);
+
+/* One estimation epoch, enqueued on the context stream (asynchronous).
+ * beat_order: B beat indices, or NULL for the library's seeded shuffle.
+ * batch_index: in/out batch-wise metric cursor (algorithm.rs:126).
+ * Device-side failures are reported by ct_sync. */
+int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, int grad_mode, int precision);
+
+/* Forward of every beat with the current parameters (no noise); writes the predicted
+ * measurements [B,T,M] and, if non-NULL, the states [T,S] of the last beat. Synchronous. */
+int ct_simulate(ct_scn* scn, float* measurements_out, float* states_out);
+
+int ct_set_algorithm(ct_scn* scn, const ct_algorithm* algo);
+int ct_set_freeze(ct_scn* scn, int freeze_gains, int freeze_delays);
+int ct_set_learning_rate(ct_scn* scn, float learning_rate);
+
+/* Field access (synchronous). nbytes must equal the field size. */
+int ct_field_size(ct_scn* scn, int field, size_t* nbytes);
+int ct_read_field(ct_scn* scn, int field, void* dst, size_t nbytes);
+int ct_write_field(ct_scn* scn, int field, const void* src, size_t nbytes);
+
+/* Waits for the context stream and reports device-side failures (e.g. CT_ERR_TIMEOUT). */
+int ct_sync(ct_scn* scn);
+
+/* Phases of the epoch timed by ct_set_profiling. */
+enum ct_phase {
+  CT_PHASE_FORWARD = 0,        /* propagation kernel */
+  CT_PHASE_MEASURE = 1,        /* H x, residuals, per-step MSE */
+  CT_PHASE_MAP_RESIDUALS = 2,  /* H^T r */
+  CT_PHASE_DERIVE = 3,         /* derivative sweep */
+  CT_PHASE_STEP_METRICS = 4,   /* running max-regularisation sum, per-step loss */
+  CT_PHASE_UPDATE = 5,         /* average delays, smoothness, optimizer, roll, batch metrics */
+  CT_PHASE_COUNT = 6
+};
+/* Kernel launches issued by this scenario since creation (host-side counter; no CUDA
+ * equivalent in the reference, which issues ~15 launches per step, gpu/epoch.rs:107-112). */
+int ct_kernel_launches(ct_scn* scn, int64_t* launches);
+/* Enable (1) / disable (0) CUDA-event timing of every phase; enabling clears the totals. */
+int ct_set_profiling(ct_scn* scn, int enable);
+/* Accumulated device milliseconds and launch counts per phase (arrays of CT_PHASE_COUNT).
+ * Synchronizes the context stream. */
+int ct_read_profile(ct_scn* scn, double* ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CARDIOTRUST_CUDA_H */

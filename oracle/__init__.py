@@ -1,0 +1,238 @@
+"""CPU restatement of the reference estimation epoch — the parity checker.
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
+and the CPU-baseline leg of ``bench.py``; never by the product package.
+
+``oracle.cpp`` follows ``src/core/algorithm.rs:124-281`` and the step
+functions it calls (file:line citations inside). :class:`OracleEpoch` owns a
+Results-like set of numpy arrays for one scenario and runs epochs on them in
+f32 (reference rounding) or f64.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+_HERE = pathlib.Path(__file__).resolve().parent
+_BUILD = _HERE / "_build"
+_LIB_PATH = _BUILD / "liboracle.so"
+_lib = None
+
+CXXFLAGS = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math", "-std=c++17", "-shared", "-fPIC"]
+
+
+def build(force: bool = False) -> pathlib.Path:
+    """Compile oracle.cpp into oracle/_build/liboracle.so (g++)."""
+    src = _HERE / "oracle.cpp"
+    if force or not _LIB_PATH.exists() or _LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+        _BUILD.mkdir(exist_ok=True)
+        tmp = _LIB_PATH.with_suffix(f".{os.getpid()}.tmp")
+        subprocess.check_call(["g++", *CXXFLAGS, str(src), "-o", str(tmp)])
+        os.replace(tmp, _LIB_PATH)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(str(_LIB_PATH))
+        _lib.oracle_from_samples_to_coef.restype = ctypes.c_float
+        _lib.oracle_from_samples_to_coef.argtypes = [ctypes.c_float]
+        _lib.oracle_from_coef_to_samples.restype = ctypes.c_float
+        _lib.oracle_from_coef_to_samples.argtypes = [ctypes.c_float]
+    return _lib
+
+
+class Algo(ctypes.Structure):
+    """Fields of the reference ``Algorithm`` config the epoch reads (config/algorithm.rs:25-58)."""
+
+    _fields_ = [
+        ("optimizer", ctypes.c_int32),
+        ("ap_derivative", ctypes.c_int32),
+        ("freeze_gains", ctypes.c_int32),
+        ("freeze_delays", ctypes.c_int32),
+        ("batch_size", ctypes.c_int64),
+        ("learning_rate", ctypes.c_float),
+        ("mse_strength", ctypes.c_float),
+        ("maximum_regularization_strength", ctypes.c_float),
+        ("maximum_regularization_threshold", ctypes.c_float),
+        ("difference_regularization_strength", ctypes.c_float),
+        ("smoothness_regularization_strength", ctypes.c_float),
+    ]
+
+
+_P = ctypes.c_void_p
+_EPOCH_FIELDS = [
+    ("num_states", ctypes.c_int64),
+    ("num_voxels", ctypes.c_int64),
+    ("num_sensors", ctypes.c_int64),
+    ("num_steps", ctypes.c_int64),
+    ("num_beats", ctypes.c_int64),
+    ("num_batch_slots", ctypes.c_int64),
+] + [
+    (name, _P)
+    for name in (
+        "gains output_state_indices coefs delays initial_delays measurement_matrix control_matrix "
+        "control_function_values actual_measurements ap_outputs_now ap_outputs_last system_states measurements "
+        "residuals average_delays d_gains d_coefs coefs_iir coefs_fir mapped_residuals maximum_regularization "
+        "maximum_regularization_sum step gains_first_moment gains_second_moment coefs_first_moment "
+        "coefs_second_moment loss loss_mse loss_maximum_regularization loss_batch loss_mse_batch "
+        "loss_maximum_regularization_batch mapped_residuals_override mapped_residuals_history"
+    ).split()
+]
+
+
+class _EpochStruct(ctypes.Structure):
+    _fields_ = _EPOCH_FIELDS
+
+
+class OracleEpoch:
+    """One scenario's model + Results arrays, run by the CPU restatement.
+
+    ``dtype`` is np.float32 (reference rounding) or np.float64.
+    """
+
+    def __init__(
+        self,
+        gains,
+        output_state_indices,
+        coefs,
+        delays,
+        initial_delays,
+        measurement_matrix,
+        control_matrix,
+        control_function,
+        actual_measurements=None,
+        num_batch_slots: int = 1,
+        dtype=np.float32,
+        keep_mapped_residuals: bool = False,
+    ):
+        self.dtype = np.dtype(dtype)
+        f = lambda a: np.ascontiguousarray(np.asarray(a), dtype=self.dtype).copy()  # noqa: E731
+        i32 = lambda a: np.ascontiguousarray(np.asarray(a), dtype=np.int32).copy()  # noqa: E731
+        self.gains = f(gains)
+        self.output_state_indices = i32(output_state_indices)
+        self.coefs = f(coefs)
+        self.delays = i32(delays)
+        self.initial_delays = f(initial_delays)
+        self.measurement_matrix = f(measurement_matrix)
+        self.control_matrix = f(control_matrix)
+        self.control_function_values = f(control_function)
+        B, M, S = self.measurement_matrix.shape
+        T = self.control_function_values.shape[0]
+        V = S // 3
+        self.num_states, self.num_voxels, self.num_sensors, self.num_steps, self.num_beats = S, V, M, T, B
+        if actual_measurements is None:
+            actual_measurements = np.zeros((B, T, M))
+        self.actual_measurements = f(actual_measurements)
+        z = lambda *shape: np.zeros(shape, dtype=self.dtype)  # noqa: E731
+        self.ap_outputs_now = z(S, 78)
+        self.ap_outputs_last = z(S, 78)
+        self.system_states = z(T, S)
+        self.measurements = z(B, T, M)
+        self.residuals = z(M)
+        self.average_delays = np.full(V, np.nan, dtype=self.dtype)
+        self.d_gains = z(S, 78)
+        self.d_coefs = z(V, 26)
+        self.coefs_iir = z(S, 78)
+        self.coefs_fir = z(S, 78)
+        self.mapped_residuals = z(S)
+        self.maximum_regularization = z(S)
+        self.maximum_regularization_sum = z(1)
+        self.step = np.ones(1, dtype=np.int64)
+        self.gains_first_moment = z(S, 78)
+        self.gains_second_moment = z(S, 78)
+        self.coefs_first_moment = z(V, 26)
+        self.coefs_second_moment = z(V, 26)
+        self.loss = z(T)
+        self.loss_mse = z(T)
+        self.loss_maximum_regularization = z(T)
+        self.num_batch_slots = int(num_batch_slots)
+        self.loss_batch = z(num_batch_slots)
+        self.loss_mse_batch = z(num_batch_slots)
+        self.loss_maximum_regularization_batch = z(num_batch_slots)
+        self.mapped_residuals_override = None
+        self.mapped_residuals_history = z(B, T, S) if keep_mapped_residuals else None
+        self.batch_index = 0
+
+    def _struct(self) -> _EpochStruct:
+        s = _EpochStruct()
+        for name, ctype in _EPOCH_FIELDS:
+            val = getattr(self, name)
+            if ctype is _P:
+                setattr(s, name, None if val is None else val.ctypes.data)
+            else:
+                setattr(s, name, int(val))
+        return s
+
+    def run_epoch(self, algo: Algo, beat_order=None) -> None:
+        """One call of ``run_epoch`` (algorithm.rs:124-281)."""
+        s = self._struct()
+        order = None
+        if beat_order is not None:
+            order = np.ascontiguousarray(beat_order, dtype=np.int32)
+        bi = ctypes.c_int64(self.batch_index)
+        fn = lib().oracle_run_epoch_f32 if self.dtype == np.float32 else lib().oracle_run_epoch_f64
+        rc = fn(
+            ctypes.byref(s),
+            ctypes.byref(algo),
+            None if order is None else order.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            ctypes.byref(bi),
+        )
+        if rc != 0:
+            raise RuntimeError(f"oracle run_epoch failed with status {rc}")
+        self.batch_index = bi.value
+
+    def simulate(self) -> np.ndarray:
+        """Forward of every beat (simulation.rs:129-150); returns measurements [B,T,M]."""
+        s = self._struct()
+        fn = lib().oracle_simulate_f32 if self.dtype == np.float32 else lib().oracle_simulate_f64
+        fn(ctypes.byref(s))
+        return self.measurements.copy()
+
+
+def algo(**kw) -> Algo:
+    """An Algo with the reference defaults (config/algorithm.rs:59-85), overridden by ``kw``."""
+    a = Algo()
+    defaults = dict(
+        optimizer=0,
+        ap_derivative=1,
+        freeze_gains=0,
+        freeze_delays=1,
+        batch_size=0,
+        learning_rate=200.0,
+        mse_strength=1.0,
+        maximum_regularization_strength=1.0,
+        maximum_regularization_threshold=1.01,
+        difference_regularization_strength=0.0,
+        smoothness_regularization_strength=0.0,
+    )
+    defaults.update(kw)
+    for k, v in defaults.items():
+        setattr(a, k, v)
+    return a
+
+
+def from_scenario(scn, dtype=np.float32, num_batch_slots: int = 1, truth: bool = False, **kw) -> OracleEpoch:
+    """OracleEpoch over a :class:`cardiotrust_b200.scenario.Scenario` (model or truth parameters)."""
+    p = scn.truth if truth else scn.model
+    return OracleEpoch(
+        p.gains,
+        p.output_state_indices,
+        p.coefs,
+        p.delays,
+        p.initial_delays,
+        scn.measurement_matrix,
+        scn.control_matrix,
+        scn.control_function,
+        scn.measurements,
+        num_batch_slots=num_batch_slots,
+        dtype=dtype,
+        **kw,
+    )

@@ -1,0 +1,675 @@
+// CPU restatement of the CardioTrust estimation epoch (`run_epoch`).
+//
+// TEST INFRASTRUCTURE ONLY. This file is the parity checker for the CUDA
+// library: it is loaded by tests/, by __graft_entry__.smoke() and by the
+// CPU-baseline leg of bench.py, and by nothing else. The product path never
+// links or calls it.
+//
+// Every function follows one function of the reference crate, cited by
+// file:line relative to the crate root. The f32 instantiation keeps the
+// reference's loop order and rounding: `a.mul_add(b, c)` becomes std::fma,
+// every other `a * b + c` is two rounded operations (the file is compiled
+// with -ffp-contract=off). The f64 instantiation is the same code in double
+// precision, used for error reports.
+//
+// Third-party arithmetic on the path (not vendored in the reference tree):
+//   * ndarray 0.16.1 `ArrayBase::dot` (matrix x vector) -> `unrolled_dot`,
+//     an eight-accumulator dot product, used by predict_measurements;
+//   * ndarray 0.16.1 `sum` -> `unrolled_fold`, same eight-accumulator shape,
+//     used by the MSE metric and the batch means;
+//   * ndarray 0.16.1 `general_mat_mul` -> matrixmultiply 0.3.10 `sgemm`,
+//     whose x86-64 FMA micro-kernel accumulates each output element with
+//     fused multiply-adds in k order inside blocks of KC = 256 and adds the
+//     blocks to C in order; used by calculate_mapped_residuals.
+// These are restated from the crates' published algorithms; their exact
+// summation order is not pinned by any test in the reference tree, so the
+// GPU is compared against these products with a tolerance, never bitwise.
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+constexpr int kOffsets = 26;
+constexpr int kGainCols = 78;
+
+struct Algo {
+  int32_t optimizer;       // 0 = Sgd, 1 = Adam           (refinement.rs:8-12)
+  int32_t ap_derivative;   // 0 = Simple, 1 = Textbook    (config/algorithm.rs:17-21)
+  int32_t freeze_gains;
+  int32_t freeze_delays;
+  int64_t batch_size;
+  float learning_rate;
+  float mse_strength;
+  float maximum_regularization_strength;
+  float maximum_regularization_threshold;
+  float difference_regularization_strength;
+  float smoothness_regularization_strength;
+};
+
+// Model + Results, as raw arrays owned by the caller. Field names follow the
+// reference structs (APParameters allpass.rs:29-36, Estimations
+// estimation.rs:24-36, Derivatives derivation.rs:31-58, Metrics
+// metrics.rs:20-37). Every float pointer has the instantiation's type T.
+template <typename T>
+struct Epoch {
+  int64_t num_states, num_voxels, num_sensors, num_steps, num_beats, num_batch_slots;
+  // model
+  T* gains;                           // [S,78]
+  const int32_t* output_state_indices;  // [S,78], -1 = None
+  T* coefs;                           // [V,26]
+  int32_t* delays;                    // [V,26]
+  const T* initial_delays;            // [V,26]
+  const T* measurement_matrix;        // [B,M,S]
+  const T* control_matrix;            // [S]
+  const T* control_function_values;   // [T]
+  const T* actual_measurements;       // [B,T,M]
+  // estimations
+  T* ap_outputs_now;   // [S,78]
+  T* ap_outputs_last;  // [S,78]
+  T* system_states;    // [T,S]
+  T* measurements;     // [B,T,M]
+  T* residuals;        // [M]
+  T* average_delays;   // [V], NaN = None
+  // derivatives
+  T* d_gains;          // [S,78]
+  T* d_coefs;          // [V,26]
+  T* coefs_iir;        // [S,78]
+  T* coefs_fir;        // [S,78]
+  T* mapped_residuals; // [S]
+  T* maximum_regularization;  // [S]
+  T* maximum_regularization_sum;  // [1]
+  int64_t* step;       // [1], starts at 1
+  T* gains_first_moment;   // [S,78] (Adam)
+  T* gains_second_moment;  // [S,78]
+  T* coefs_first_moment;   // [V,26]
+  T* coefs_second_moment;  // [V,26]
+  // metrics
+  T* loss;       // [T]
+  T* loss_mse;   // [T]
+  T* loss_maximum_regularization;  // [T]
+  T* loss_batch;       // [num_batch_slots]
+  T* loss_mse_batch;
+  T* loss_maximum_regularization_batch;
+  // optional: mapped residuals per (beat, step) [B,T,S] used instead of H^T r
+  const T* mapped_residuals_override;
+  // optional: receives H^T r per (beat, step) [B,T,S]
+  T* mapped_residuals_history;
+};
+
+// ---------------------------------------------------------------- ndarray / matrixmultiply
+
+template <typename T>
+T unrolled_dot(const T* xs, const T* ys, int64_t n) {
+  T sum = 0, p0 = 0, p1 = 0, p2 = 0, p3 = 0, p4 = 0, p5 = 0, p6 = 0, p7 = 0;
+  int64_t i = 0;
+  for (; n - i >= 8; i += 8) {
+    p0 = p0 + xs[i + 0] * ys[i + 0];
+    p1 = p1 + xs[i + 1] * ys[i + 1];
+    p2 = p2 + xs[i + 2] * ys[i + 2];
+    p3 = p3 + xs[i + 3] * ys[i + 3];
+    p4 = p4 + xs[i + 4] * ys[i + 4];
+    p5 = p5 + xs[i + 5] * ys[i + 5];
+    p6 = p6 + xs[i + 6] * ys[i + 6];
+    p7 = p7 + xs[i + 7] * ys[i + 7];
+  }
+  sum = sum + (p0 + p4);
+  sum = sum + (p1 + p5);
+  sum = sum + (p2 + p6);
+  sum = sum + (p3 + p7);
+  for (int64_t j = 0; i < n && j < 7; ++i, ++j) sum = sum + xs[i] * ys[i];
+  return sum;
+}
+
+template <typename T>
+T unrolled_sum(const T* xs, int64_t n) {
+  T acc = 0, p0 = 0, p1 = 0, p2 = 0, p3 = 0, p4 = 0, p5 = 0, p6 = 0, p7 = 0;
+  int64_t i = 0;
+  for (; n - i >= 8; i += 8) {
+    p0 = p0 + xs[i + 0];
+    p1 = p1 + xs[i + 1];
+    p2 = p2 + xs[i + 2];
+    p3 = p3 + xs[i + 3];
+    p4 = p4 + xs[i + 4];
+    p5 = p5 + xs[i + 5];
+    p6 = p6 + xs[i + 6];
+    p7 = p7 + xs[i + 7];
+  }
+  acc = acc + (p0 + p4);
+  acc = acc + (p1 + p5);
+  acc = acc + (p2 + p6);
+  acc = acc + (p3 + p7);
+  for (int64_t j = 0; i < n && j < 7; ++i, ++j) acc = acc + xs[i];
+  return acc;
+}
+
+template <typename T>
+T mean(const T* xs, int64_t n) {
+  return unrolled_sum(xs, n) / static_cast<T>(n);
+}
+
+// ---------------------------------------------------------------- allpass helpers
+
+template <typename T>
+T from_coef_to_samples(T coef) {  // allpass.rs:661-665
+  return (T(1) - coef) / (coef + T(1));
+}
+
+float from_samples_to_coef_f32(float samples) {  // allpass.rs:640-646
+  float fractional = std::fmod(samples, 1.0f);
+  float coef = (1.0f - fractional) / (1.0f + fractional);
+  if (coef < 1e-4f) coef = 1e-4f;
+  if (coef > 1.0f - 1e-4f) coef = 1.0f - 1e-4f;
+  return coef;
+}
+
+template <typename T>
+T powi5(T x) {  // f32::powi(5): x * ((x*x)*(x*x))
+  T x2 = x * x;
+  T x4 = x2 * x2;
+  return x * x4;
+}
+
+template <typename T>
+T signum(T x) {  // f32::signum: +-1 with the sign bit of x, NaN for NaN
+  if (std::isnan(x)) return x;
+  return std::copysign(T(1), x);
+}
+
+// ---------------------------------------------------------------- prediction
+
+// innovate_system_states_v1, estimation/prediction.rs:40-86
+template <typename T>
+void innovate_system_states(Epoch<T>& e, int64_t step) {
+  const int64_t S = e.num_states;
+  std::memcpy(e.ap_outputs_last, e.ap_outputs_now, sizeof(T) * S * kGainCols);
+  T* x_now = e.system_states + step * S;
+  for (int64_t i = 0; i < S; ++i) {
+    for (int k = 0; k < kGainCols; ++k) {
+      const int32_t out = e.output_state_indices[i * kGainCols + k];
+      if (out < 0) continue;
+      const int64_t ci = (i / 3) * kOffsets + k / 3;
+      const T coef = e.coefs[ci];
+      const int64_t delay = e.delays[ci];
+      const T input = (delay <= step) ? e.system_states[(step - delay) * S + out] : T(0);
+      const T input_delayed = (delay < step) ? e.system_states[(step - delay - 1) * S + out] : T(0);
+      T& ap = e.ap_outputs_now[i * kGainCols + k];
+      ap = std::fma(coef, input - ap, input_delayed);
+      x_now[i] += e.gains[i * kGainCols + k] * ap;
+    }
+  }
+}
+
+// add_control_function, prediction.rs:94-106 (ndarray scaled_add: y = y + alpha * x)
+template <typename T>
+void add_control_function(Epoch<T>& e, int64_t step) {
+  const int64_t S = e.num_states;
+  const T u = e.control_function_values[step];
+  T* x_now = e.system_states + step * S;
+  for (int64_t i = 0; i < S; ++i) x_now[i] = x_now[i] + u * e.control_matrix[i];
+}
+
+// predict_measurements, prediction.rs:112-130
+template <typename T>
+void predict_measurements(Epoch<T>& e, int64_t beat, int64_t step) {
+  const int64_t S = e.num_states, M = e.num_sensors, Tn = e.num_steps;
+  const T* H = e.measurement_matrix + beat * M * S;
+  const T* x = e.system_states + step * S;
+  T* y = e.measurements + (beat * Tn + step) * M;
+  for (int64_t m = 0; m < M; ++m) y[m] = unrolled_dot(H + m * S, x, S) * T(1);
+}
+
+// calculate_residuals, estimation.rs:146-153
+template <typename T>
+void calculate_residuals(Epoch<T>& e, int64_t beat, int64_t step) {
+  const int64_t M = e.num_sensors, Tn = e.num_steps;
+  const T* y = e.measurements + (beat * Tn + step) * M;
+  const T* z = e.actual_measurements + (beat * Tn + step) * M;
+  for (int64_t m = 0; m < M; ++m) e.residuals[m] = y[m] - z[m];
+}
+
+// ---------------------------------------------------------------- derivation
+
+// calculate_mapped_residuals, derivation.rs:538-551 (matrixmultiply sgemm, n = 1)
+template <typename T>
+void calculate_mapped_residuals(Epoch<T>& e, int64_t beat, int64_t step) {
+  const int64_t S = e.num_states, M = e.num_sensors, Tn = e.num_steps;
+  if (e.mapped_residuals_override) {
+    std::memcpy(e.mapped_residuals, e.mapped_residuals_override + (beat * Tn + step) * S, sizeof(T) * S);
+  } else {
+    const T* H = e.measurement_matrix + beat * M * S;
+    constexpr int64_t KC = 256;
+    for (int64_t s = 0; s < S; ++s) {
+      T c = 0;
+      for (int64_t k0 = 0; k0 < M; k0 += KC) {
+        const int64_t k1 = (k0 + KC < M) ? k0 + KC : M;
+        T ab = 0;
+        for (int64_t m = k0; m < k1; ++m) ab = std::fma(H[m * S + s], e.residuals[m], ab);
+        c = (k0 == 0) ? ab : ab + c;
+      }
+      e.mapped_residuals[s] = c;
+    }
+  }
+  if (e.mapped_residuals_history)
+    std::memcpy(e.mapped_residuals_history + (beat * Tn + step) * S, e.mapped_residuals, sizeof(T) * S);
+}
+
+// calculate_maximum_regularization, derivation.rs:509-535
+template <typename T>
+void calculate_maximum_regularization(Epoch<T>& e, int64_t step, T threshold) {
+  const int64_t S = e.num_states;
+  const T* x = e.system_states + step * S;
+  T* mr = e.maximum_regularization;
+  for (int64_t i = 0; i < S; i += 3) {
+    const T sum = std::fabs(x[i]) + std::fabs(x[i + 1]) + std::fabs(x[i + 2]);
+    if (sum > threshold) {
+      const T factor = sum - threshold;
+      *e.maximum_regularization_sum += factor * factor;
+      mr[i] = factor * signum(x[i]);
+      mr[i + 1] = factor * signum(x[i + 1]);
+      mr[i + 2] = factor * signum(x[i + 2]);
+    } else {
+      mr[i] = 0;
+      mr[i + 1] = 0;
+      mr[i + 2] = 0;
+    }
+  }
+}
+
+// calculate_derivatives_gains, derivation.rs:307-329
+template <typename T>
+void calculate_derivatives_gains(Epoch<T>& e, const Algo& a) {
+  const int64_t S = e.num_states;
+  const T mse_scaling = T(1) / static_cast<T>(e.num_sensors) * static_cast<T>(a.mse_strength);
+  const T reg_scaling = static_cast<T>(a.maximum_regularization_strength);
+  for (int64_t i = 0; i < S; ++i) {
+    const T max_reg = e.maximum_regularization[i];
+    const T residual = e.mapped_residuals[i];
+    for (int k = 0; k < kGainCols; ++k) {
+      const T ap = e.ap_outputs_now[i * kGainCols + k];
+      e.d_gains[i * kGainCols + k] += ap * std::fma(residual, mse_scaling, max_reg * reg_scaling);
+    }
+  }
+}
+
+template <typename T>
+T delay_delta(const Epoch<T>& e, int64_t ci) {
+  const T delay = static_cast<T>(e.delays[ci]) + from_coef_to_samples(e.coefs[ci]);
+  return powi5(e.initial_delays[ci] - delay);
+}
+
+// calculate_derivatives_coefs_simple, derivation.rs:338-398
+template <typename T>
+void calculate_derivatives_coefs_simple(Epoch<T>& e, int64_t step, const Algo& a) {
+  const int64_t S = e.num_states;
+  const T mse_scaling = T(1) / static_cast<T>(e.num_sensors) * static_cast<T>(a.mse_strength);
+  const T diff = static_cast<T>(a.difference_regularization_strength);
+  for (int64_t i = 0; i < S; ++i) {
+    for (int k = 0; k < kGainCols; ++k) {
+      const int64_t ci = (i / 3) * kOffsets + k / 3;
+      const T dd = delay_delta(e, ci);
+      const int32_t out = e.output_state_indices[i * kGainCols + k];
+      if (out < 0) continue;
+      const int64_t delay = e.delays[ci];
+      if (step >= delay) {
+        const T ap_last = e.ap_outputs_last[i * kGainCols + k];
+        const T state_val = e.system_states[(step - delay) * S + out];
+        const T g = e.gains[i * kGainCols + k];
+        const T mr = e.mapped_residuals[i];
+        e.d_coefs[ci] += std::fma((state_val - ap_last) * g * mr, mse_scaling, diff * dd);
+      }
+    }
+  }
+}
+
+// calculate_derivatives_coefs_textbook, derivation.rs:408-501
+template <typename T>
+void calculate_derivatives_coefs_textbook(Epoch<T>& e, int64_t step, const Algo& a) {
+  const int64_t S = e.num_states;
+  const T mse_scaling = T(1) / static_cast<T>(e.num_sensors) * static_cast<T>(a.mse_strength);
+  const T diff = static_cast<T>(a.difference_regularization_strength);
+  for (int64_t i = 0; i < S; ++i) {
+    for (int k = 0; k < kGainCols; ++k) {
+      const int32_t out = e.output_state_indices[i * kGainCols + k];
+      if (out < 0) continue;
+      const int64_t ci = (i / 3) * kOffsets + k / 3;
+      const int64_t delay = e.delays[ci];
+      if (step >= delay) {
+        const T state_val = e.system_states[(step - delay) * S + out];
+        T& fir = e.coefs_fir[i * kGainCols + k];
+        fir = std::fma(-e.coefs[ci], fir, state_val);
+      }
+    }
+  }
+  for (int64_t i = 0; i < S; ++i) {
+    for (int k = 0; k < kGainCols; ++k) {
+      const int64_t ci = (i / 3) * kOffsets + k / 3;
+      const int64_t delay = e.delays[ci];
+      if (step >= delay) {
+        T& iir = e.coefs_iir[i * kGainCols + k];
+        iir = std::fma(-e.coefs[ci], iir, e.ap_outputs_last[i * kGainCols + k]);
+      }
+    }
+  }
+  for (int64_t i = 0; i < S; ++i) {
+    for (int k = 0; k < kGainCols; ++k) {
+      const int64_t ci = (i / 3) * kOffsets + k / 3;
+      const T dd = delay_delta(e, ci);
+      const T iir = e.coefs_iir[i * kGainCols + k];
+      const T fir = e.coefs_fir[i * kGainCols + k];
+      const T g = e.gains[i * kGainCols + k];
+      const T mr = e.mapped_residuals[i];
+      e.d_coefs[ci] += std::fma((fir - iir) * g * mr, mse_scaling, diff * dd);
+    }
+  }
+}
+
+// calculate_step_derivatives, derivation.rs:173-229
+template <typename T>
+void calculate_step_derivatives(Epoch<T>& e, const Algo& a, int64_t step, int64_t beat) {
+  calculate_mapped_residuals(e, beat, step);
+  calculate_maximum_regularization(e, step, static_cast<T>(a.maximum_regularization_threshold));
+  if (!a.freeze_gains) calculate_derivatives_gains(e, a);
+  if (!a.freeze_delays) {
+    if (a.ap_derivative == 0)
+      calculate_derivatives_coefs_simple(e, step, a);
+    else
+      calculate_derivatives_coefs_textbook(e, step, a);
+  }
+}
+
+// calculate_average_delays, derivation.rs:554-594
+template <typename T>
+void calculate_average_delays(Epoch<T>& e) {
+  static const int kOff[26][3] = {
+      {-1, -1, -1}, {-1, -1, 0}, {-1, -1, 1}, {-1, 0, -1}, {-1, 0, 0}, {-1, 0, 1}, {-1, 1, -1},
+      {-1, 1, 0},   {-1, 1, 1},  {0, -1, -1}, {0, -1, 0},  {0, -1, 1}, {0, 0, -1},  {0, 0, 1},
+      {0, 1, -1},   {0, 1, 0},   {0, 1, 1},   {1, -1, -1}, {1, -1, 0}, {1, -1, 1},  {1, 0, -1},
+      {1, 0, 0},    {1, 0, 1},   {1, 1, -1},  {1, 1, 0},   {1, 1, 1}};
+  for (int64_t v = 0; v < e.num_voxels; ++v) {
+    T delay_sum = 0, gain_sum = 0;
+    for (int n = 0; n < kOffsets; ++n) {
+      const int xyz = std::abs(kOff[n][0]) + std::abs(kOff[n][1]) + std::abs(kOff[n][2]);
+      const int64_t ci = v * kOffsets + n;
+      const T delay = static_cast<T>(e.delays[ci]) + from_coef_to_samples(e.coefs[ci]);
+      const T corrected = delay / std::sqrt(static_cast<T>(xyz));
+      for (int in = 0; in < 3; ++in)
+        for (int out = 0; out < 3; ++out) {
+          const T g = e.gains[(v * 3 + in) * kGainCols + n * 3 + out];
+          delay_sum += std::fabs(g) * corrected;
+          gain_sum += std::fabs(g);
+        }
+    }
+    e.average_delays[v] = (gain_sum == T(0)) ? T(NAN) : delay_sum / gain_sum;
+  }
+}
+
+// calculate_smoothness_derivatives, derivation.rs:260-302
+template <typename T>
+void calculate_smoothness_derivatives(Epoch<T>& e, const Algo& a) {
+  for (int64_t v = 0; v < e.num_voxels; ++v) {
+    for (int n_out = 0; n_out < kOffsets; ++n_out) {
+      const T own = e.average_delays[v];
+      if (std::isnan(own)) continue;
+      T neighbourhood = own;
+      T divisor = 1;
+      for (int n = 0; n < kOffsets; ++n) {
+        const int32_t nb = e.output_state_indices[(v * 3) * kGainCols + n * 3];
+        if (nb < 0) continue;
+        const T d = e.average_delays[nb / 3];
+        if (!std::isnan(d)) {
+          neighbourhood += d;
+          divisor += 1;
+        }
+      }
+      neighbourhood /= divisor;
+      e.d_coefs[v * kOffsets + n_out] += static_cast<T>(a.smoothness_regularization_strength) * (neighbourhood - own);
+    }
+  }
+}
+
+// calculate_batch_derivatives, derivation.rs:241-256
+template <typename T>
+void calculate_batch_derivatives(Epoch<T>& e, const Algo& a) {
+  if (!a.freeze_delays && std::fabs(a.smoothness_regularization_strength) > 1.1920929e-7f)
+    calculate_smoothness_derivatives(e, a);
+}
+
+// Derivatives::reset, derivation.rs:114-122
+template <typename T>
+void derivatives_reset(Epoch<T>& e) {
+  const int64_t S = e.num_states, V = e.num_voxels;
+  std::fill(e.d_gains, e.d_gains + S * kGainCols, T(0));
+  std::fill(e.d_coefs, e.d_coefs + V * kOffsets, T(0));
+  std::fill(e.coefs_iir, e.coefs_iir + S * kGainCols, T(0));
+  std::fill(e.coefs_fir, e.coefs_fir + S * kGainCols, T(0));
+  std::fill(e.maximum_regularization, e.maximum_regularization + S, T(0));
+  *e.maximum_regularization_sum = 0;
+}
+
+// ---------------------------------------------------------------- update
+
+template <typename T>
+struct AdamConsts {
+  T beta1, one_minus_beta1, beta2, one_minus_beta2, epsilon, bias1, bias2;
+};
+
+template <typename T>
+AdamConsts<T> adam_consts(int64_t step) {  // update.rs:129-141 (f32 constants, powf from libm)
+  AdamConsts<T> c;
+  c.beta1 = static_cast<T>(0.9f);
+  c.one_minus_beta1 = T(1) - c.beta1;
+  c.beta2 = static_cast<T>(0.999f);
+  c.one_minus_beta2 = T(1) - c.beta2;
+  c.epsilon = static_cast<T>(1e-8f);
+  c.bias1 = T(1) - std::pow(c.beta1, static_cast<T>(static_cast<float>(step)));
+  c.bias2 = T(1) - std::pow(c.beta2, static_cast<T>(static_cast<float>(step)));
+  return c;
+}
+
+template <typename T>
+void adam(T* p, const T* g, T* m, T* v, int64_t n, const AdamConsts<T>& c, T lr_over_bs) {
+  for (int64_t i = 0; i < n; ++i) {  // update.rs:136-145 / 190-199
+    m[i] = m[i] * c.beta1 + c.one_minus_beta1 * g[i];
+    v[i] = v[i] * c.beta2 + c.one_minus_beta2 * g[i] * g[i];
+    const T mc = m[i] / c.bias1;
+    const T vc = v[i] / c.bias2;
+    const T factor = mc / (std::sqrt(vc) + c.epsilon);
+    p[i] = p[i] - lr_over_bs * factor;
+  }
+}
+
+template <typename T>
+void sgd(T* p, const T* g, int64_t n, T lr_over_bs) {  // update.rs:106-114 / 158-168
+  for (int64_t i = 0; i < n; ++i) p[i] = p[i] - lr_over_bs * g[i];
+}
+
+// roll_delays, update.rs:206-228
+template <typename T>
+void roll_delays(T* coefs, int32_t* delays, int64_t n) {
+  const T margin = static_cast<T>(1e-4f);
+  for (int64_t i = 0; i < n; ++i) {
+    T& c = coefs[i];
+    int32_t& d = delays[i];
+    if (c > T(1) - margin) {
+      if (d > 1) {
+        c = T(2) * margin;
+        d -= 1;
+      } else {
+        c = T(1) - margin;
+      }
+    } else if (c < margin) {
+      if (d < 1000) {
+        c = std::fma(T(2), -margin, T(1));
+        d += 1;
+      } else {
+        c = margin;
+      }
+    }
+  }
+}
+
+// APParameters::update, update.rs:27-97
+template <typename T>
+void ap_update(Epoch<T>& e, const Algo& a, int64_t num_steps, int64_t num_beats) {
+  const int64_t S = e.num_states, V = e.num_voxels;
+  const int64_t bs = (a.batch_size == 0) ? num_steps * num_beats : num_steps * a.batch_size;
+  const T lr_over_bs = static_cast<T>(a.learning_rate) / static_cast<T>(static_cast<float>(bs));
+  if (!a.freeze_gains) {
+    if (a.optimizer == 0)
+      sgd(e.gains, e.d_gains, S * kGainCols, lr_over_bs);
+    else
+      adam(e.gains, e.d_gains, e.gains_first_moment, e.gains_second_moment, S * kGainCols,
+           adam_consts<T>(*e.step), lr_over_bs);
+  }
+  if (!a.freeze_delays) {
+    if (a.optimizer == 0)
+      sgd(e.coefs, e.d_coefs, V * kOffsets, lr_over_bs);
+    else
+      adam(e.coefs, e.d_coefs, e.coefs_first_moment, e.coefs_second_moment, V * kOffsets,
+           adam_consts<T>(*e.step), lr_over_bs);
+    roll_delays(e.coefs, e.delays, V * kOffsets);
+  }
+  *e.step += 1;
+}
+
+// ---------------------------------------------------------------- metrics
+
+// metrics::calculate_step, metrics.rs:180-196
+template <typename T>
+void metrics_step(Epoch<T>& e, T reg_strength, int64_t step) {
+  const int64_t M = e.num_sensors;
+  std::vector<T> sq(M);
+  for (int64_t m = 0; m < M; ++m) sq[m] = e.residuals[m] * e.residuals[m];
+  e.loss_mse[step] = unrolled_sum(sq.data(), M) / static_cast<T>(M);
+  e.loss_maximum_regularization[step] = *e.maximum_regularization_sum;
+  e.loss[step] = std::fma(reg_strength, e.loss_maximum_regularization[step], e.loss_mse[step]);
+}
+
+// metrics::calculate_batch, metrics.rs:204-219
+template <typename T>
+int metrics_batch(Epoch<T>& e, int64_t index) {
+  if (index < 0 || index >= e.num_batch_slots) return -3;
+  const int64_t Tn = e.num_steps;
+  e.loss_mse_batch[index] = mean(e.loss_mse, Tn);
+  e.loss_maximum_regularization_batch[index] = mean(e.loss_maximum_regularization, Tn);
+  e.loss_batch[index] = mean(e.loss, Tn);
+  return 0;
+}
+
+// ---------------------------------------------------------------- epoch
+
+// Estimations::reset, estimation.rs:82-87
+template <typename T>
+void estimations_reset(Epoch<T>& e) {
+  std::fill(e.system_states, e.system_states + e.num_steps * e.num_states, T(0));
+  std::fill(e.ap_outputs_now, e.ap_outputs_now + e.num_states * kGainCols, T(0));
+}
+
+// calculate_system_prediction, prediction.rs:15-26
+template <typename T>
+void system_prediction(Epoch<T>& e, int64_t beat, int64_t step) {
+  innovate_system_states(e, step);
+  add_control_function(e, step);
+  predict_measurements(e, beat, step);
+}
+
+template <typename T>
+int batch_end(Epoch<T>& e, const Algo& a, int64_t n, int64_t* batch_index) {
+  calculate_average_delays(e);
+  calculate_batch_derivatives(e, a);
+  ap_update(e, a, e.num_steps, n);
+  int rc = metrics_batch(e, *batch_index);
+  *batch_index += 1;
+  return rc;
+}
+
+// run_epoch, algorithm.rs:124-281. The beat order is an input (the reference
+// shuffles with an unseeded generator, algorithm.rs:139-141).
+template <typename T>
+int run_epoch(Epoch<T>& e, const Algo& a, const int32_t* beat_order, int64_t* batch_index) {
+  derivatives_reset(e);
+  const T reg = static_cast<T>(a.maximum_regularization_strength);
+  int64_t batch = 0;
+  const bool batched = a.batch_size != 0;
+  for (int64_t bi = 0; bi < e.num_beats; ++bi) {
+    const int64_t beat = beat_order ? beat_order[bi] : bi;
+    if (beat < 0 || beat >= e.num_beats) return -2;
+    estimations_reset(e);
+    for (int64_t step = 0; step < e.num_steps; ++step) {
+      system_prediction(e, beat, step);
+      calculate_residuals(e, beat, step);
+      calculate_step_derivatives(e, a, step, beat);
+      metrics_step(e, reg, step);
+    }
+    if (batched) {
+      batch += 1;
+      if (batch == a.batch_size) {
+        int rc = batch_end(e, a, batch, batch_index);
+        if (rc) return rc;
+        derivatives_reset(e);
+        batch = 0;
+      }
+    }
+  }
+  if (batched) {
+    if (batch > 0) return batch_end(e, a, batch, batch_index);
+    return 0;
+  }
+  return batch_end(e, a, e.num_beats, batch_index);
+}
+
+// Simulation::run forward part, data/simulation.rs:129-150: every beat's
+// system prediction; states of the last beat stay in system_states.
+template <typename T>
+void simulate(Epoch<T>& e) {
+  for (int64_t beat = 0; beat < e.num_beats; ++beat) {
+    estimations_reset(e);
+    for (int64_t step = 0; step < e.num_steps; ++step) system_prediction(e, beat, step);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_abi_version() { return 1; }
+
+int oracle_run_epoch_f32(Epoch<float>* e, const Algo* a, const int32_t* beat_order, int64_t* batch_index) {
+  return run_epoch(*e, *a, beat_order, batch_index);
+}
+int oracle_run_epoch_f64(Epoch<double>* e, const Algo* a, const int32_t* beat_order, int64_t* batch_index) {
+  return run_epoch(*e, *a, beat_order, batch_index);
+}
+int oracle_simulate_f32(Epoch<float>* e) {
+  simulate(*e);
+  return 0;
+}
+int oracle_simulate_f64(Epoch<double>* e) {
+  simulate(*e);
+  return 0;
+}
+
+// Single-step entry points for known-answer tests.
+float oracle_from_samples_to_coef(float s) { return from_samples_to_coef_f32(s); }
+float oracle_from_coef_to_samples(float c) { return from_coef_to_samples(c); }
+int oracle_average_delays_f32(Epoch<float>* e) {
+  calculate_average_delays(*e);
+  return 0;
+}
+void oracle_sgd_f32(float* p, const float* g, int64_t n, float lr, int64_t bs) {
+  sgd(p, g, n, lr / static_cast<float>(bs));
+}
+void oracle_adam_f32(float* p, const float* g, float* m, float* v, int64_t n, int64_t step, float lr, int64_t bs) {
+  adam(p, g, m, v, n, adam_consts<float>(step), lr / static_cast<float>(bs));
+}
+void oracle_roll_delays_f32(float* c, int32_t* d, int64_t n) { roll_delays(c, d, n); }
+void oracle_adam_bias_f32(int64_t step, float* out2) {
+  AdamConsts<float> c = adam_consts<float>(step);
+  out2[0] = c.bias1;
+  out2[1] = c.bias2;
+}
+
+}  // extern "C"
