@@ -221,7 +221,10 @@ def gpu_arm(args):
     from cardiotrust_b200 import algorithm as alg
     from cardiotrust_b200 import scenario as sc
 
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library issues every kernel on it, and the timing events,
+    # the L2 flush and the barriers below are ordered on it too
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx = alg.Context(local_rank, stream=stream.cuda_stream)
     scn = sc.build(sc.workload_spec(args.workload, seed=rank))
     # ground truth with the CUDA forward (Simulation::run reuses the prediction path)

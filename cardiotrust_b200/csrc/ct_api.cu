@@ -23,11 +23,14 @@ using ct::DeviceScenario;
 using ct::kGainCols;
 using ct::kOffsets;
 
+// A context lives until the caller has destroyed it and every scenario created
+// on it is gone (reference count: one for the caller, one per scenario).
 struct ct_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int num_sms = 0;
+  int refs = 1;
 };
 
 struct PhaseEvents {
@@ -374,11 +377,18 @@ int ct_ctx_create(int device, void* stream, ct_ctx** out) {
   return CT_OK;
 }
 
-int ct_ctx_destroy(ct_ctx* ctx) {
-  if (!ctx) return CT_OK;
+namespace {
+void ctx_release(ct_ctx* ctx) {
+  if (--ctx->refs > 0) return;
   cudaSetDevice(ctx->device);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+}
+}  // namespace
+
+int ct_ctx_destroy(ct_ctx* ctx) {
+  if (!ctx) return CT_OK;
+  ctx_release(ctx);
   return CT_OK;
 }
 
@@ -528,16 +538,19 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
     delete s;
     return r;
   }
+  ctx->refs += 1;
   *out = s;
   return CT_OK;
 }
 
 int ct_scenario_destroy(ct_scn* scn) {
   if (!scn) return CT_OK;
-  cudaSetDevice(scn->ctx->device);
-  cudaStreamSynchronize(scn->ctx->stream);
+  ct_ctx* ctx = scn->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
   free_scenario(scn);
   delete scn;
+  ctx_release(ctx);
   return CT_OK;
 }
 

@@ -80,24 +80,47 @@ __global__ void __launch_bounds__(128) derive_kernel(DeriveArgs p) {
   const bool do_gains = !p.s.freeze_gains, do_coefs = !p.s.freeze_delays;
   const bool textbook = p.s.ap_derivative != 0;
 
+  // Step t needs x[t-d] (all-pass input, fir input), x[t-d-1] (= the input of step t-1),
+  // x[t, 3v..3v+2] and mr[t, 3v..3v+2]. The loads of step t+1 are issued before the
+  // arithmetic of step t (two-stage software pipeline).
+  const float* xv = p.X + 3 * v;
+  const float* mrv = p.MR + 3 * v;
+  float in_prev[3] = {0.0f, 0.0f, 0.0f};
+  float nin[3], nx[3], nmr[3];
+#pragma unroll
+  for (int b = 0; b < 3; ++b) nin[b] = (valid && d <= 0) ? __ldg(p.X + j0 + b) : 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    nx[a] = __ldg(xv + a);
+    nmr[a] = __ldg(mrv + a);
+  }
   for (int64_t t = 0; t < T; ++t) {
-    float ap_last[3], in[3];
+    float in[3], x[3], mr[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      in[q] = nin[q];
+      x[q] = nx[q];
+      mr[q] = nmr[q];
+    }
+    if (t + 1 < T) {
+      const int64_t tn = t + 1;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) nin[b] = (valid && d <= tn) ? __ldg(p.X + (tn - d) * S + j0 + b) : 0.0f;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        nx[a] = __ldg(xv + tn * S + a);
+        nmr[a] = __ldg(mrv + tn * S + a);
+      }
+    }
+    float ap_last[3];
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
       ap_last[b] = ap[b];
-      in[b] = 0.0f;
-      if (valid) {
-        in[b] = (d <= t) ? __ldg(p.X + (t - d) * S + j0 + b) : 0.0f;
-        const float in1 = (d < t) ? __ldg(p.X + (t - d - 1) * S + j0 + b) : 0.0f;
-        ap[b] = fmaf(c, in[b] - ap[b], in1);
-      }
+      // in_prev = x[t-d-1] (zero while t-d-1 < 0), prediction.rs:73-77
+      if (valid) ap[b] = fmaf(c, in[b] - ap[b], in_prev[b]);
+      in_prev[b] = in[b];
     }
-    float x[3], mr[3], mreg[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      x[a] = __ldg(p.X + t * S + 3 * v + a);
-      mr[a] = __ldg(p.MR + t * S + 3 * v + a);
-    }
+    float mreg[3];
     const float sum = fabsf(x[0]) + fabsf(x[1]) + fabsf(x[2]);
     const bool over = sum > thr;
     const float f = sum - thr;

@@ -21,8 +21,9 @@
 //     all-pass chain and stages the L outputs in shared memory.
 //     Phase B: one thread per (voxel, row component, step parity) sums the 78
 //     gain-weighted outputs in column order k = 0..77 for its steps.
-//   * History reads use ld.global.cg (L2): the rows were written by other SMs
-//     before the last grid barrier.
+//   * History reads go through L1: within one launch a history row is read
+//     only after the grid barrier that completes it, so no SM can hold a
+//     stale line of it (L1 holds no global data across launches).
 #include <cuda_runtime.h>
 
 #include "ct_internal.cuh"
@@ -89,13 +90,21 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(FwdArgs p) {
           const int64_t j = 3 * (int64_t)nb + b;
           const int64_t d = p.delays[v * kOffsets + n];
           const float c = p.coefs[v * kOffsets + n];
-          for (int s = 0; s < L; ++s) {
-            const int64_t t = t0 + s;
-            const float in = (d <= t) ? __ldcg(p.X + (t - d) * S + j) : 0.0f;
-            const float in1 = (d < t) ? __ldcg(p.X + (t - d - 1) * S + j) : 0.0f;
-            a = fmaf(c, in - a, in1);
-            sm_ap[s * (kTileVoxels * kGainCols) + item] = a;
-            if (t == T - 2) p.ap_last[v * kGainCols + kk] = a;
+          // h[q] = x[t0 - d - 1 + q, j]: in(t0+s) = h[s+1], in_delayed(t0+s) = h[s]; rows before
+          // t = 0 read as zero (prediction.rs:68-77). All loads are independent and issued together.
+          float h[kMaxStepBlock + 1];
+#pragma unroll
+          for (int q = 0; q <= kMaxStepBlock; ++q) {
+            const int64_t tr = t0 - d - 1 + q;
+            h[q] = (q <= L && tr >= 0) ? p.X[tr * S + j] : 0.0f;
+          }
+#pragma unroll
+          for (int s = 0; s < kMaxStepBlock; ++s) {
+            if (s < L) {
+              a = fmaf(c, h[s + 1] - a, h[s]);
+              sm_ap[s * (kTileVoxels * kGainCols) + item] = a;
+              if (t0 + s == T - 2) p.ap_last[v * kGainCols + kk] = a;
+            }
           }
         } else {
           for (int s = 0; s < L; ++s) sm_ap[s * (kTileVoxels * kGainCols) + item] = 0.0f;
@@ -208,6 +217,8 @@ cudaError_t launch_forward(DeviceScenario& d, float threshold, cudaStream_t stre
   a.status = d.status;
   a.barrier = d.barrier;
   cudaError_t err = cudaMemsetAsync(d.ap, 0, sizeof(float) * d.V * kGainCols, stream);
+  if (err != cudaSuccess) return err;
+  err = cudaMemsetAsync(d.ap_last, 0, sizeof(float) * d.V * kGainCols, stream);
   if (err != cudaSuccess) return err;
   err = cudaMemsetAsync(d.barrier, 0, sizeof(GridBarrier), stream);
   if (err != cudaSuccess) return err;

@@ -136,7 +136,8 @@ const char* ct_status_string(int status);
 int ct_last_error(char* buf, size_t len);
 
 /* Context = device + stream. stream == NULL creates a private non-blocking stream;
- * otherwise the context issues all work on the given cudaStream_t. */
+ * otherwise the context issues all work on the given cudaStream_t. A destroyed context
+ * stays alive until the last scenario created on it is destroyed. */
 int ct_ctx_create(int device, void* stream, ct_ctx** out);
 int ct_ctx_destroy(ct_ctx* ctx);
 int ct_ctx_stream(ct_ctx* ctx, void** stream);

@@ -194,7 +194,8 @@ def test_batches_and_beat_order(alg, ctx, oracle_mod):
     bi = eng.run_epoch(0, beat_order=order)
     o.run_epoch(oa, beat_order=order)
     assert bi == o.batch_index == 2
-    assert_bitwise(eng.read("system_states"), o.system_states, "system_states")
+    # the last beat runs after the in-loop update, whose parameters agree within the gradient tolerance
+    assert rel_err(eng.read("system_states"), o.system_states) < TOL_LOSS
     assert rel_err(eng.read("measurements"), o.measurements) < 10 * TOL_MEAS
     assert rel_err(eng.read("loss_batch"), o.loss_batch) < TOL_LOSS
     g0 = scn.model.gains.astype(np.float64)
