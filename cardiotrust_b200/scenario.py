@@ -296,33 +296,27 @@ def _output_state_indices(types: np.ndarray, numbers: np.ndarray) -> np.ndarray:
 def _delay_samples(types, numbers, positions, velocity, sample_rate) -> np.ndarray:
     """calculate_delay_samples_array (delay.rs:35-111) for a uniform velocity.
 
-    Every neighbour pair of a regular grid has one of three distances, so the
-    delay depends only on the offset; it is evaluated once per offset with the
-    f32 arithmetic of delay.rs:14-23 and written where the neighbour exists.
+    Every neighbour pair with the same offset has the same distance on a
+    regular grid (positions are exact multiples of the voxel size), so the
+    delay is evaluated once per offset, on the first voxel that has that
+    neighbour, with the f32 arithmetic of delay.rs:14-23.
     """
     nbr = _neighbour_table(numbers)
     V = nbr.shape[0]
     out = np.zeros((V, 26), dtype=np.float32)
-    p0 = positions[0, 0, 0]
-    nx, ny, nz = numbers.shape
+    coords = np.argwhere(numbers >= 0)  # numbering order
     for n in range(26):
-        ox, oy, oz = delay_index_to_offset(n)
-        # a reference pair with the same offset (positions are uniform, so any pair gives the same bits
-        # only if the coordinates are exact; the grid positions are small multiples of 2.5 mm)
-        base = np.array([1, 1, 1]) if min(nx, ny, nz) > 2 else np.array([0, 0, 0])
-        samples = None
-        if all(0 <= base[d] + o < s for d, (o, s) in enumerate(zip((ox, oy, oz), (nx, ny, nz)))):
-            pin = positions[tuple(base)]
-            pout = positions[tuple(base + np.array([ox, oy, oz]))]
-            samples = np.float32(_delay_s(pin, pout, velocity) * np.float32(sample_rate))
         has = nbr[:, n] >= 0
-        if has.any():
-            if samples is None:
-                raise ValueError("grid too small for the offset table")
-            if samples < 1.0:
-                raise ValueError(f"delay below one sample: {samples}")
-            out[has, n] = samples
-    _ = p0
+        if not has.any():
+            continue
+        v = int(np.argmax(has))
+        ox, oy, oz = delay_index_to_offset(n)
+        x, y, z = coords[v]
+        samples = np.float32(_delay_s(positions[x, y, z], positions[x + ox, y + oy, z + oz], velocity)
+                             * np.float32(sample_rate))
+        if samples < 1.0:
+            raise ValueError(f"delay below one sample: {samples}")
+        out[has, n] = samples
     return out
 
 
