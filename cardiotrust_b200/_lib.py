@@ -83,6 +83,7 @@ EXPORTED = [
     "ct_kernel_launches",
     "ct_set_profiling",
     "ct_read_profile",
+    "ct_predict_measurements_noalloc",
 ]
 
 PHASES = ["forward", "measure", "map_residuals", "derive", "step_metrics", "update"]
@@ -165,6 +166,8 @@ def load(path: pathlib.Path = LIB_PATH) -> ctypes.CDLL:
     lib.ct_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     lib.ct_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.ct_read_profile.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+    lib.ct_predict_measurements_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int64, ctypes.c_int64,
+                                                    ctypes.c_int64, vp]
     for name in EXPORTED:
         getattr(lib, name)  # AttributeError if a declared symbol is not exported
     return lib

@@ -329,6 +329,10 @@ int copy_down_expanded(ct_scn* s, float* dst, const float* src) {
 
 }  // namespace
 
+namespace ct {
+int report_error(int status, const char* message) { return fail(status, "%s", message); }
+}  // namespace ct
+
 extern "C" {
 
 int ct_version(void) { return CT_ABI_VERSION; }

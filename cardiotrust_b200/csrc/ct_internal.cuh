@@ -63,6 +63,9 @@ struct DeviceScenario {
   GridBarrier* barrier;  // [1]
 };
 
+// Records `message` as the calling thread's last error (read by ct_last_error); returns status.
+int report_error(int status, const char* message);
+
 // ---- launchers (all enqueue on `stream`, return cudaError_t of the launch)
 
 // Forward propagation of one beat: X[t,:] for t in [0,T).

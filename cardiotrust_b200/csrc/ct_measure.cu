@@ -11,6 +11,9 @@
 // partials are summed in a fixed order.
 #include <cuda_runtime.h>
 
+#include <cstdio>
+#include <mutex>
+
 #include "ct_internal.cuh"
 
 namespace ct {
@@ -142,4 +145,96 @@ cudaError_t launch_map_residuals(DeviceScenario& d, int64_t beat, cudaStream_t s
   return cudaGetLastError();
 }
 
+// ---- allocation-free variant of the H x product -------------------------------------------
+//
+// For callers that must not see device allocations from this library: hosts
+// that place every device buffer in their own pool or arena, or run under a
+// fixed device-memory budget, and callers for which the implicit device
+// synchronisation of cudaMalloc / cudaFree is not acceptable. The split-K
+// partial sums live in one file-scope device array instead of a per-scenario
+// cudaMalloc'd buffer. Every GPU that loads the library holds this array
+// (8 MiB) until the process exits.
+
+namespace {
+
+constexpr int64_t kStaticScratchFloats = int64_t(1) << 21;  // 2,097,152 floats = 8 MiB
+__device__ __align__(256) float g_measure_scratch[kStaticScratchFloats];
+
+constexpr int kMaxDevices = 128;
+std::mutex g_scratch_mutex;
+float* g_scratch_address[kMaxDevices] = {};
+
+// Device address of g_measure_scratch on the current device. In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device with that device current, and cached.
+int scratch_address(int device, float** out) {
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_address[device]) {
+    void* p = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&p, g_measure_scratch);
+    if (err != cudaSuccess) {
+      char msg[256];
+      std::snprintf(msg, sizeof(msg), "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(err));
+      return report_error(CT_ERR_CUDA, msg);
+    }
+    g_scratch_address[device] = static_cast<float*>(p);
+  }
+  *out = g_scratch_address[device];
+  return CT_OK;
+}
+
+}  // namespace
 }  // namespace ct
+
+extern "C" int ct_predict_measurements_noalloc(const float* states, const float* measurement_matrix,
+                                               const float* actual, float* predicted, float* residuals,
+                                               int64_t num_steps, int64_t num_states, int64_t num_sensors,
+                                               void* stream) {
+  using namespace ct;
+  if (!states || !measurement_matrix || !predicted)
+    return report_error(CT_ERR_INVALID_ARGUMENT, "states, measurement_matrix and predicted must be device pointers");
+  if (residuals && !actual) return report_error(CT_ERR_INVALID_ARGUMENT, "residuals need the actual measurements");
+  const int64_t T = num_steps, S = num_states, M = num_sensors;
+  if (T <= 0 || S <= 0 || M <= 0) return report_error(CT_ERR_INVALID_ARGUMENT, "num_steps, num_states and num_sensors must be positive");
+  const int64_t mpad = ((M + BN - 1) / BN) * BN;
+  if (T * mpad > kStaticScratchFloats) {
+    char msg[256];
+    std::snprintf(msg, sizeof(msg),
+                  "num_steps x ceil64(num_sensors) = %lld x %lld exceeds the static scratch of %lld floats",
+                  (long long)T, (long long)mpad, (long long)kStaticScratchFloats);
+    return report_error(CT_ERR_INVALID_ARGUMENT, msg);
+  }
+  int device = 0;
+  cudaError_t err = cudaGetDevice(&device);
+  if (err != cudaSuccess || device < 0 || device >= kMaxDevices)
+    return report_error(CT_ERR_CUDA, "cudaGetDevice failed or device index out of range");
+  float* scratch = nullptr;
+  int rc = scratch_address(device, &scratch);
+  if (rc) return rc;
+  int sms = 0;
+  err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (err != cudaSuccess) return report_error(CT_ERR_CUDA, "cudaDeviceGetAttribute failed");
+  // split-K factor: as for the scenario path, but bounded by the scratch capacity
+  const int64_t tiles = ((M + BN - 1) / BN) * ((T + BM - 1) / BM);
+  int64_t ks = (2 * (int64_t)sms + tiles - 1) / tiles;
+  const int64_t by_k = S / 256 > 1 ? S / 256 : 1;
+  const int64_t by_scratch = kStaticScratchFloats / (T * mpad);
+  if (ks > by_k) ks = by_k;
+  if (ks > 64) ks = 64;
+  if (ks > by_scratch) ks = by_scratch;
+  if (ks < 1) ks = 1;
+  const int64_t kchunk = ((S + ks - 1) / ks + BK - 1) / BK * BK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // every (split, step, sensor) partial read below is written first, so nothing is cleared
+  dim3 grid((unsigned)((M + BN - 1) / BN), (unsigned)((T + BM - 1) / BM), (unsigned)ks);
+  gemm_kernel<true><<<grid, kThreads, 0, st>>>(states, S, measurement_matrix, S, scratch, mpad, T * mpad, T, M, S,
+                                               kchunk);
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return report_error(CT_ERR_CUDA, cudaGetErrorString(err));
+  const int64_t n = T * M;
+  reduce_measure_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(scratch, (int)ks, T, M, mpad, predicted,
+                                                                    residuals ? actual : nullptr, residuals);
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return report_error(CT_ERR_CUDA, cudaGetErrorString(err));
+  return CT_OK;
+}

@@ -188,6 +188,24 @@ int ct_set_profiling(ct_scn* scn, int enable);
  * Synchronizes the context stream. */
 int ct_read_profile(ct_scn* scn, double* ms, int64_t* launches);
 
+/* Allocation-free H x product for callers that must not see this library allocate device
+ * memory: hosts that keep every device buffer in their own pool or arena or run under a fixed
+ * memory budget, and callers that cannot accept the implicit device synchronisation of
+ * cudaMalloc / cudaFree. No counterpart in the reference crate.
+ *
+ * predicted[t, m] = sum_s measurement_matrix[m, s] * states[t, s] for one beat, and, when
+ * residuals is non-NULL, residuals = predicted - actual (all [T, M]). All pointers are device
+ * pointers owned by the caller; work is enqueued on `stream` (NULL = legacy default stream).
+ * Split-K partial sums go to one 8 MiB file-scope device array that every GPU loading the
+ * library holds until exit; num_steps x ceil(num_sensors / 64) x 64 must not exceed 2,097,152
+ * (CT_ERR_INVALID_ARGUMENT otherwise). The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current; make that first call before any
+ * stream capture. The function calls no cudaMalloc / cudaFree. All calls share the array:
+ * calls that overlap on the GPU (other streams, other host threads) race on it. */
+int ct_predict_measurements_noalloc(const float* states, const float* measurement_matrix, const float* actual,
+                                    float* predicted, float* residuals, int64_t num_steps, int64_t num_states,
+                                    int64_t num_sensors, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
