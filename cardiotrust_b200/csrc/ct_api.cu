@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <tuple>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -45,7 +46,9 @@ struct ct_scn {
   int64_t adam_step = 1;  // Derivatives.step, derivation.rs:100
   uint64_t rng = 0x9e3779b97f4a7c15ull;
   std::vector<void*> allocations;
-  std::vector<int32_t> nbr_host;  // neighbour table, for validating delay writes
+  std::vector<int32_t> nbr_host;  // neighbour table in reference order, for validating delay writes
+  // Device voxel order: device voxel u holds reference voxel perm[u]; inv is the inverse.
+  std::vector<int32_t> perm, inv;
   // launch accounting and optional per-phase CUDA-event timing
   int64_t launches = 0;
   bool profiling = false;
@@ -228,6 +231,112 @@ int batch_end(ct_scn* s, int64_t n_beats, int64_t* batch_index) {
   return CT_OK;
 }
 
+// ---- device voxel order --------------------------------------------------------------
+//
+// Kernels see the voxels in spatially compact 4x4x2 bricks, so the 26
+// neighbours of a tile of consecutive device voxels are few and close, and
+// their state history is reused from L1. Integer grid coordinates are
+// recovered from the neighbour table (offset index n <-> (dx, dy, dz), the
+// ordering of delay_index_to_offset, allpass.rs:597-611) by a breadth-first
+// walk; each connected component is laid out on its own. Any permutation is
+// correct (every per-state operation and its order is unchanged); the bricks
+// only improve locality. Arrays cross the ABI in reference order.
+
+const int kOffsetXYZ[kOffsets][3] = {
+    {-1, -1, -1}, {-1, -1, 0}, {-1, -1, 1}, {-1, 0, -1}, {-1, 0, 0}, {-1, 0, 1}, {-1, 1, -1},
+    {-1, 1, 0},   {-1, 1, 1},  {0, -1, -1}, {0, -1, 0},  {0, -1, 1}, {0, 0, -1},  {0, 0, 1},
+    {0, 1, -1},   {0, 1, 0},   {0, 1, 1},   {1, -1, -1}, {1, -1, 0}, {1, -1, 1},  {1, 0, -1},
+    {1, 0, 0},    {1, 0, 1},   {1, 1, -1},  {1, 1, 0},   {1, 1, 1}};
+
+void brick_layout(const std::vector<int32_t>& nbr, int64_t V, std::vector<int32_t>& perm,
+                  std::vector<int32_t>& inv) {
+  std::vector<int64_t> cx((size_t)V), cy((size_t)V), cz((size_t)V), comp((size_t)V, -1);
+  std::vector<int32_t> queue;
+  queue.reserve((size_t)V);
+  int64_t ncomp = 0;
+  for (int64_t root = 0; root < V; ++root) {
+    if (comp[(size_t)root] >= 0) continue;
+    queue.clear();
+    queue.push_back((int32_t)root);
+    comp[(size_t)root] = ncomp;
+    cx[(size_t)root] = cy[(size_t)root] = cz[(size_t)root] = 0;
+    for (size_t qi = 0; qi < queue.size(); ++qi) {
+      const int32_t u = queue[qi];
+      for (int n = 0; n < kOffsets; ++n) {
+        const int32_t w = nbr[(size_t)u * kOffsets + n];
+        if (w < 0 || comp[(size_t)w] >= 0) continue;
+        comp[(size_t)w] = ncomp;
+        cx[(size_t)w] = cx[(size_t)u] + kOffsetXYZ[n][0];
+        cy[(size_t)w] = cy[(size_t)u] + kOffsetXYZ[n][1];
+        cz[(size_t)w] = cz[(size_t)u] + kOffsetXYZ[n][2];
+        queue.push_back(w);
+      }
+    }
+    // shift the component to non-negative coordinates
+    int64_t mx = 0, my = 0, mz = 0;
+    for (int32_t u : queue) {
+      mx = std::min(mx, cx[(size_t)u]);
+      my = std::min(my, cy[(size_t)u]);
+      mz = std::min(mz, cz[(size_t)u]);
+    }
+    for (int32_t u : queue) {
+      cx[(size_t)u] -= mx;
+      cy[(size_t)u] -= my;
+      cz[(size_t)u] -= mz;
+    }
+    ++ncomp;
+  }
+  perm.resize((size_t)V);
+  for (int64_t v = 0; v < V; ++v) perm[(size_t)v] = (int32_t)v;
+  auto key = [&](int32_t v) {
+    return std::make_tuple(comp[(size_t)v], cx[(size_t)v] / 4, cy[(size_t)v] / 4, cz[(size_t)v] / 2,
+                           cx[(size_t)v], cy[(size_t)v], cz[(size_t)v], v);
+  };
+  std::sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) { return key(a) < key(b); });
+  inv.resize((size_t)V);
+  for (int64_t u = 0; u < V; ++u) inv[(size_t)perm[(size_t)u]] = (int32_t)u;
+}
+
+// Row blocks of `rows_per_voxel` rows of `row_len` elements: device block u <- reference block perm[u].
+template <typename T>
+void gather_rows(T* dst, const T* src, const std::vector<int32_t>& perm, int64_t rows_per_voxel, int64_t row_len) {
+  const size_t blk = (size_t)(rows_per_voxel * row_len);
+  for (size_t u = 0; u < perm.size(); ++u) std::memcpy(dst + u * blk, src + (size_t)perm[u] * blk, sizeof(T) * blk);
+}
+// Inverse of gather_rows: reference block perm[u] <- device block u.
+template <typename T>
+void scatter_rows(T* dst, const T* src, const std::vector<int32_t>& perm, int64_t rows_per_voxel, int64_t row_len) {
+  const size_t blk = (size_t)(rows_per_voxel * row_len);
+  for (size_t u = 0; u < perm.size(); ++u) std::memcpy(dst + (size_t)perm[u] * blk, src + u * blk, sizeof(T) * blk);
+}
+// Columns of `rows` rows of S = 3V states: device state 3u+a <- reference state 3perm[u]+a.
+void gather_state_columns(float* dst, const float* src, const std::vector<int32_t>& perm, int64_t rows) {
+  const size_t S = 3 * perm.size();
+  for (int64_t r = 0; r < rows; ++r) {
+    const float* sr = src + (size_t)r * S;
+    float* dr = dst + (size_t)r * S;
+    for (size_t u = 0; u < perm.size(); ++u) {
+      const size_t v = (size_t)perm[u];
+      dr[3 * u] = sr[3 * v];
+      dr[3 * u + 1] = sr[3 * v + 1];
+      dr[3 * u + 2] = sr[3 * v + 2];
+    }
+  }
+}
+void scatter_state_columns(float* dst, const float* src, const std::vector<int32_t>& perm, int64_t rows) {
+  const size_t S = 3 * perm.size();
+  for (int64_t r = 0; r < rows; ++r) {
+    const float* sr = src + (size_t)r * S;
+    float* dr = dst + (size_t)r * S;
+    for (size_t u = 0; u < perm.size(); ++u) {
+      const size_t v = (size_t)perm[u];
+      dr[3 * v] = sr[3 * u];
+      dr[3 * v + 1] = sr[3 * u + 1];
+      dr[3 * v + 2] = sr[3 * u + 2];
+    }
+  }
+}
+
 int validate_and_build_nbr(const ct_scenario_desc* desc, std::vector<int32_t>& nbr) {
   const int64_t S = desc->num_states, V = S / 3;
   nbr.assign((size_t)(V * kOffsets), -1);
@@ -315,15 +424,36 @@ int copy_down(ct_scn* s, void* dst, const void* src, size_t bytes) {
   return CT_OK;
 }
 
-// [V,78] device -> [S,78] host (row component replicated)
+// [V,78] device order -> [S,78] reference order (row component replicated)
 int copy_down_expanded(ct_scn* s, float* dst, const float* src) {
   const int64_t V = s->d.V;
   std::vector<float> tmp((size_t)(V * kGainCols));
   int rc = copy_down(s, tmp.data(), src, sizeof(float) * tmp.size());
   if (rc) return rc;
-  for (int64_t v = 0; v < V; ++v)
+  for (int64_t u = 0; u < V; ++u) {
+    const int64_t v = s->perm[(size_t)u];
     for (int a = 0; a < 3; ++a)
-      std::memcpy(dst + (3 * v + a) * kGainCols, tmp.data() + v * kGainCols, sizeof(float) * kGainCols);
+      std::memcpy(dst + (3 * v + a) * kGainCols, tmp.data() + u * kGainCols, sizeof(float) * kGainCols);
+  }
+  return CT_OK;
+}
+
+// Per-voxel row blocks (rows_per_voxel x row_len elements) in device order -> reference order.
+template <typename T>
+int copy_down_rows(ct_scn* s, T* dst, const T* src, int64_t rows_per_voxel, int64_t row_len) {
+  std::vector<T> tmp((size_t)(s->d.V * rows_per_voxel * row_len));
+  int rc = copy_down(s, tmp.data(), src, sizeof(T) * tmp.size());
+  if (rc) return rc;
+  scatter_rows(dst, tmp.data(), s->perm, rows_per_voxel, row_len);
+  return CT_OK;
+}
+
+// `rows` rows of S states in device order -> reference order.
+int copy_down_state_columns(ct_scn* s, float* dst, const float* src, int64_t rows) {
+  std::vector<float> tmp((size_t)(rows * s->d.S));
+  int rc = copy_down(s, tmp.data(), src, sizeof(float) * tmp.size());
+  if (rc) return rc;
+  scatter_state_columns(dst, tmp.data(), s->perm, rows);
   return CT_OK;
 }
 
@@ -411,6 +541,8 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   if (S <= 0 || S % 3 != 0) return fail(CT_ERR_INVALID_ARGUMENT, "num_states %lld must be a positive multiple of 3", (long long)S);
   if (M <= 0 || T <= 0 || B <= 0) return fail(CT_ERR_INVALID_ARGUMENT, "num_sensors, num_steps and num_beats must be positive");
   if (desc->num_batch_slots <= 0) return fail(CT_ERR_INVALID_ARGUMENT, "num_batch_slots must be positive");
+  if (T * S >= (int64_t(1) << 31) || S * kGainCols >= (int64_t(1) << 31) || B * M * S >= (int64_t(1) << 40))
+    return fail(CT_ERR_NOT_SUPPORTED, "num_steps x num_states must stay below 2^31 (32-bit state indexing)");
   if (!desc->gains || !desc->output_state_indices || !desc->coefs || !desc->delays || !desc->initial_delays ||
       !desc->measurement_matrix || !desc->control_matrix || !desc->control_function)
     return fail(CT_ERR_INVALID_ARGUMENT, "a required array pointer is NULL");
@@ -423,6 +555,7 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   s->ctx = ctx;
   s->algo = *algo;
   s->nbr_host = nbr;
+  brick_layout(nbr, S / 3, s->perm, s->inv);
   DeviceScenario& d = s->d;
   d.S = S;
   d.V = S / 3;
@@ -486,13 +619,29 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
 #undef ALLOC
   cudaStream_t st = ctx->stream;
   int r = CT_OK;
-  r = r ? r : upload(s, d.gains, desc->gains, sizeof(float) * S * kGainCols);
-  r = r ? r : upload(s, d.nbr, nbr.data(), sizeof(int32_t) * V * kOffsets);
-  r = r ? r : upload(s, d.coefs, desc->coefs, sizeof(float) * V * kOffsets);
-  r = r ? r : upload(s, d.delays, desc->delays, sizeof(int32_t) * V * kOffsets);
-  r = r ? r : upload(s, d.init_delays, desc->initial_delays, sizeof(float) * V * kOffsets);
-  r = r ? r : upload(s, d.H, desc->measurement_matrix, sizeof(float) * B * M * S);
-  r = r ? r : upload(s, d.ctrl, desc->control_matrix, sizeof(float) * S);
+  // model arrays in device voxel order (uploads are synchronous on the context stream below,
+  // so the host staging vectors outlive their copies)
+  std::vector<float> h_gains((size_t)(S * kGainCols)), h_coefs((size_t)(V * kOffsets)),
+      h_init((size_t)(V * kOffsets)), h_ctrl((size_t)S), h_H((size_t)(B * M * S));
+  std::vector<int32_t> h_nbr((size_t)(V * kOffsets)), h_delays((size_t)(V * kOffsets));
+  gather_rows(h_gains.data(), desc->gains, s->perm, 3, kGainCols);
+  gather_rows(h_coefs.data(), desc->coefs, s->perm, 1, kOffsets);
+  gather_rows(h_init.data(), desc->initial_delays, s->perm, 1, kOffsets);
+  gather_rows(h_delays.data(), desc->delays, s->perm, 1, kOffsets);
+  gather_state_columns(h_ctrl.data(), desc->control_matrix, s->perm, 1);
+  gather_state_columns(h_H.data(), desc->measurement_matrix, s->perm, B * M);
+  for (int64_t u = 0; u < V; ++u)
+    for (int n = 0; n < kOffsets; ++n) {
+      const int32_t w = nbr[(size_t)s->perm[(size_t)u] * kOffsets + n];
+      h_nbr[(size_t)(u * kOffsets + n)] = w < 0 ? -1 : s->inv[(size_t)w];
+    }
+  r = r ? r : upload(s, d.gains, h_gains.data(), sizeof(float) * S * kGainCols);
+  r = r ? r : upload(s, d.nbr, h_nbr.data(), sizeof(int32_t) * V * kOffsets);
+  r = r ? r : upload(s, d.coefs, h_coefs.data(), sizeof(float) * V * kOffsets);
+  r = r ? r : upload(s, d.delays, h_delays.data(), sizeof(int32_t) * V * kOffsets);
+  r = r ? r : upload(s, d.init_delays, h_init.data(), sizeof(float) * V * kOffsets);
+  r = r ? r : upload(s, d.H, h_H.data(), sizeof(float) * B * M * S);
+  r = r ? r : upload(s, d.ctrl, h_ctrl.data(), sizeof(float) * S);
   r = r ? r : upload(s, d.u, desc->control_function, sizeof(float) * T);
   if (!r && desc->measurements) r = upload(s, d.meas, desc->measurements, sizeof(float) * B * T * M);
   if (!r && !desc->measurements) {
@@ -623,7 +772,7 @@ int ct_simulate(ct_scn* scn, float* measurements_out, float* states_out) {
   if (rc) return rc;
   rc = copy_down(scn, measurements_out, d.Y, sizeof(float) * d.B * d.T * d.M);
   if (rc) return rc;
-  if (states_out) rc = copy_down(scn, states_out, d.X, sizeof(float) * d.T * d.S);
+  if (states_out) rc = copy_down_state_columns(scn, states_out, d.X, d.T);
   return rc;
 }
 
@@ -663,37 +812,37 @@ int ct_read_field(ct_scn* scn, int field, void* dst, size_t nbytes) {
   DeviceScenario& d = scn->d;
   float* out = static_cast<float*>(dst);
   switch (field) {
-    case CT_FIELD_GAINS: return copy_down(scn, dst, d.gains, nbytes);
-    case CT_FIELD_COEFS: return copy_down(scn, dst, d.coefs, nbytes);
-    case CT_FIELD_DELAYS: return copy_down(scn, dst, d.delays, nbytes);
+    case CT_FIELD_GAINS: return copy_down_rows(scn, out, d.gains, 3, kGainCols);
+    case CT_FIELD_COEFS: return copy_down_rows(scn, out, d.coefs, 1, kOffsets);
+    case CT_FIELD_DELAYS: return copy_down_rows(scn, static_cast<int32_t*>(dst), d.delays, 1, kOffsets);
     case CT_FIELD_MEASUREMENTS_ACTUAL: return copy_down(scn, dst, d.meas, nbytes);
-    case CT_FIELD_SYSTEM_STATES: return copy_down(scn, dst, d.X, nbytes);
+    case CT_FIELD_SYSTEM_STATES: return copy_down_state_columns(scn, out, d.X, d.T);
     case CT_FIELD_MEASUREMENTS: return copy_down(scn, dst, d.Y, nbytes);
     case CT_FIELD_RESIDUALS: return copy_down(scn, dst, d.R + (d.T - 1) * d.M, nbytes);
     case CT_FIELD_AP_OUTPUTS_NOW: return copy_down_expanded(scn, out, d.ap);
     case CT_FIELD_AP_OUTPUTS_LAST: return copy_down_expanded(scn, out, d.ap_last);
-    case CT_FIELD_AVERAGE_DELAYS: return copy_down(scn, dst, d.avg_delays, nbytes);
-    case CT_FIELD_GRAD_GAINS: return copy_down(scn, dst, d.dG, nbytes);
-    case CT_FIELD_GRAD_COEFS: return copy_down(scn, dst, d.dC, nbytes);
+    case CT_FIELD_AVERAGE_DELAYS: return copy_down_rows(scn, out, d.avg_delays, 1, 1);
+    case CT_FIELD_GRAD_GAINS: return copy_down_rows(scn, out, d.dG, 3, kGainCols);
+    case CT_FIELD_GRAD_COEFS: return copy_down_rows(scn, out, d.dC, 1, kOffsets);
     case CT_FIELD_COEFS_FIR: return copy_down_expanded(scn, out, d.fir);
     case CT_FIELD_COEFS_IIR: return copy_down_expanded(scn, out, d.iir);
-    case CT_FIELD_MAPPED_RESIDUALS: return copy_down(scn, dst, d.MR + (d.T - 1) * d.S, nbytes);
+    case CT_FIELD_MAPPED_RESIDUALS: return copy_down_state_columns(scn, out, d.MR + (d.T - 1) * d.S, 1);
     case CT_FIELD_MAXIMUM_REGULARIZATION: {
       // derived from the last step's states into a temporary device buffer (read-back path only)
       float* tmp = nullptr;
       CT_CUDA(cudaMallocAsync((void**)&tmp, nbytes, scn->ctx->stream), "cudaMallocAsync");
       cudaError_t e = ct::launch_last_max_reg(d, scn->algo.maximum_regularization_threshold, tmp, scn->ctx->stream);
-      int r2 = e == cudaSuccess ? copy_down(scn, dst, tmp, nbytes) : cuda_fail(e, "max reg kernel");
+      int r2 = e == cudaSuccess ? copy_down_state_columns(scn, out, tmp, 1) : cuda_fail(e, "max reg kernel");
       cudaFreeAsync(tmp, scn->ctx->stream);
       return r2;
     }
     case CT_FIELD_MAXIMUM_REGULARIZATION_SUM: return copy_down(scn, dst, d.mreg_sum, nbytes);
     case CT_FIELD_ADAM_STEP: std::memcpy(dst, &scn->adam_step, sizeof(int64_t)); return CT_OK;
-    case CT_FIELD_GAINS_FIRST_MOMENT: return copy_down(scn, dst, d.mG1, nbytes);
-    case CT_FIELD_GAINS_SECOND_MOMENT: return copy_down(scn, dst, d.mG2, nbytes);
-    case CT_FIELD_COEFS_FIRST_MOMENT: return copy_down(scn, dst, d.mC1, nbytes);
-    case CT_FIELD_COEFS_SECOND_MOMENT: return copy_down(scn, dst, d.mC2, nbytes);
-    case CT_FIELD_MAPPED_RESIDUALS_HISTORY: return copy_down(scn, dst, d.MR, nbytes);
+    case CT_FIELD_GAINS_FIRST_MOMENT: return copy_down_rows(scn, out, d.mG1, 3, kGainCols);
+    case CT_FIELD_GAINS_SECOND_MOMENT: return copy_down_rows(scn, out, d.mG2, 3, kGainCols);
+    case CT_FIELD_COEFS_FIRST_MOMENT: return copy_down_rows(scn, out, d.mC1, 1, kOffsets);
+    case CT_FIELD_COEFS_SECOND_MOMENT: return copy_down_rows(scn, out, d.mC2, 1, kOffsets);
+    case CT_FIELD_MAPPED_RESIDUALS_HISTORY: return copy_down_state_columns(scn, out, d.MR, d.T);
     case CT_FIELD_LOSS: return copy_down(scn, dst, d.loss, nbytes);
     case CT_FIELD_LOSS_MSE: return copy_down(scn, dst, d.loss_mse, nbytes);
     case CT_FIELD_LOSS_MAXIMUM_REGULARIZATION: return copy_down(scn, dst, d.loss_mr, nbytes);
@@ -728,7 +877,21 @@ int ct_write_field(ct_scn* scn, int field, const void* src, size_t nbytes) {
     case CT_FIELD_MEASUREMENTS_ACTUAL: dst = d.meas; break;
     default: return fail(CT_ERR_INVALID_ARGUMENT, "field %d is read-only", field);
   }
-  CT_CUDA(cudaMemcpyAsync(dst, src, nbytes, cudaMemcpyHostToDevice, scn->ctx->stream), "write field");
+  // reorder into device voxel order (measurements are in sensor space and need no reordering)
+  std::vector<unsigned char> staged;
+  const void* from = src;
+  if (field != CT_FIELD_MEASUREMENTS_ACTUAL) {
+    staged.resize(nbytes);
+    if (field == CT_FIELD_GAINS)
+      gather_rows(reinterpret_cast<float*>(staged.data()), static_cast<const float*>(src), scn->perm, 3, kGainCols);
+    else if (field == CT_FIELD_COEFS)
+      gather_rows(reinterpret_cast<float*>(staged.data()), static_cast<const float*>(src), scn->perm, 1, kOffsets);
+    else
+      gather_rows(reinterpret_cast<int32_t*>(staged.data()), static_cast<const int32_t*>(src), scn->perm, 1,
+                  kOffsets);
+    from = staged.data();
+  }
+  CT_CUDA(cudaMemcpyAsync(dst, from, nbytes, cudaMemcpyHostToDevice, scn->ctx->stream), "write field");
   if (field == CT_FIELD_DELAYS) CT_CUDA(ct::launch_min_delay(d, scn->ctx->stream), "min delay kernel");
   CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "write field");
   return CT_OK;
