@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--cpu-steps", type=int, default=200, help="steps of the bounded CPU sample")
+    p.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "tf32"],
+                   help="measurement products: FP32 CUDA cores, tcgen05 split TF32, tcgen05 TF32")
     return p.parse_args()
 
 
@@ -236,6 +238,7 @@ def gpu_arm(args):
     scn.measurements = (y + rng.normal(0.0, sigma, size=y.shape)).astype(np.float32)
 
     cfg = algorithm_config(alg)
+    prec = {"fp32": alg.Precision.Fp32, "tf32x3": alg.Precision.Tf32x3, "tf32": alg.Precision.Tf32}[args.precision]
     total_epochs = args.warmup + 3 * args.steps + 4
     eng = alg.EpochEngine.from_scenario(ctx, scn, num_batch_slots=total_epochs, algorithm=cfg)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
@@ -248,7 +251,7 @@ def gpu_arm(args):
 
     bi = 0
     for _ in range(args.warmup):
-        bi = eng.run_epoch(bi, sync=True)
+        bi = eng.run_epoch(bi, precision=prec, sync=True)
     barrier()
 
     # ---- device-resident timed region
@@ -259,7 +262,7 @@ def gpu_arm(args):
     for k in range(args.steps):
         flush.random_(0, 255)
         ev[k][0].record(stream)
-        bi = eng.run_epoch(bi, sync=False)
+        bi = eng.run_epoch(bi, precision=prec, sync=False)
         ev[k][1].record(stream)
     torch.cuda.synchronize()
     eng.sync()
@@ -290,7 +293,7 @@ def gpu_arm(args):
         eng.write("coefs", h_coefs)
         eng.write("delays", h_delays)
         eng.write("measurements_actual", h_meas)
-        bi = eng.run_epoch(bi, sync=True)
+        bi = eng.run_epoch(bi, precision=prec, sync=True)
         eng.read_into("gains", out_gains)
         eng.read_into("coefs", out_coefs)
         eng.read_into("delays", out_delays)
@@ -307,7 +310,7 @@ def gpu_arm(args):
     eng.set_profiling(True)
     for _ in range(args.steps):
         flush.random_(0, 255)
-        bi = eng.run_epoch(bi, sync=False)
+        bi = eng.run_epoch(bi, precision=prec, sync=False)
     prof = eng.read_profile()
     eng.set_profiling(False)
     peaks = {}
@@ -362,7 +365,7 @@ def gpu_arm(args):
                 "workload": f"{args.workload}: 20x20x20 cuboid, {V} voxels, {S} states, T={T}, "
                             f"{scn.num_sensors} sensor rows, {B} beat, Adam lr 1e-3, gains+coefficients (textbook)",
                 "voxels": V, "states": S, "steps_per_epoch": T, "beats": B, "sensor_rows": scn.num_sensors,
-                "grad_mode": "reference", "precision": "fp32",
+                "grad_mode": "reference", "precision": args.precision,
                 "l2": "256 MB buffer written between timed epochs (not timed)",
                 "parallelism": f"replicas x{world}",
             },

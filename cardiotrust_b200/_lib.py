@@ -27,6 +27,8 @@ CT_OPT_SGD, CT_OPT_ADAM = 0, 1
 CT_AP_SIMPLE, CT_AP_TEXTBOOK = 0, 1
 CT_GRAD_REFERENCE = 0
 CT_PREC_FP32 = 0
+CT_PREC_TF32X3 = 1
+CT_PREC_TF32 = 2
 
 # ct_field values with (dtype, shape-builder(S, V, M, T, B, NB))
 FIELDS = {

@@ -42,7 +42,9 @@ class GradMode(enum.IntEnum):
 
 
 class Precision(enum.IntEnum):
-    Fp32 = 0
+    Fp32 = 0  # FP32 CUDA-core GEMMs
+    Tf32x3 = 1  # tcgen05 TF32 with hi/lo operand split
+    Tf32 = 2  # tcgen05 TF32, one pass
 
 
 @dataclasses.dataclass

@@ -152,17 +152,26 @@ void seeded_shuffle(ct_scn* s, std::vector<int32_t>& order) {
   }
 }
 
-int run_beat(ct_scn* s, int64_t beat) {
+int run_beat(ct_scn* s, int64_t beat, int precision) {
   DeviceScenario& d = s->d;
   const ct_algorithm& a = s->algo;
   cudaStream_t st = s->ctx->stream;
   CT_CUDA(run_phase(s, CT_PHASE_FORWARD, 1,
                     [&] { return ct::launch_forward(d, a.maximum_regularization_threshold, st); }),
           "forward kernel");
-  CT_CUDA(run_phase(s, CT_PHASE_MEASURE, 3, [&] { return ct::launch_measure(d, beat, true, st); }),
-          "measurement kernel");
-  CT_CUDA(run_phase(s, CT_PHASE_MAP_RESIDUALS, 1, [&] { return ct::launch_map_residuals(d, beat, st); }),
-          "mapped-residual kernel");
+  if (precision == CT_PREC_FP32) {
+    CT_CUDA(run_phase(s, CT_PHASE_MEASURE, 3, [&] { return ct::launch_measure(d, beat, true, st); }),
+            "measurement kernel");
+    CT_CUDA(run_phase(s, CT_PHASE_MAP_RESIDUALS, 1, [&] { return ct::launch_map_residuals(d, beat, st); }),
+            "mapped-residual kernel");
+  } else {
+    CT_CUDA(run_phase(s, CT_PHASE_MEASURE, 3,
+                      [&] { return ct::launch_measure_umma(d, beat, true, precision, st); }),
+            "tensor-core measurement kernel");
+    CT_CUDA(run_phase(s, CT_PHASE_MAP_RESIDUALS, 1,
+                      [&] { return ct::launch_map_residuals_umma(d, beat, precision, st); }),
+            "tensor-core mapped-residual kernel");
+  }
   if (!a.freeze_gains || !a.freeze_delays) {
     ct::DeriveScalars ds;
     ds.mse_scaling = 1.0f / (float)d.M * a.mse_strength;
@@ -570,7 +579,13 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
     ks = std::min<int64_t>(ks, std::max<int64_t>(1, S / 256));
     d.ksplit = (int)std::max<int64_t>(1, std::min<int64_t>(ks, 64));
   }
+  d.umma = ct::umma_supported(S, M);
+  d.kpad = ((M + 31) / 32) * 32;
+  d.ksplit_umma = d.umma ? ct::umma_ksplit(T, S, M, ctx->num_sms) : 1;
   const int64_t V = d.V, mpad = ((M + 63) / 64) * 64;
+  const int64_t ldp_umma = ((M + ct::umma_yn(M) - 1) / ct::umma_yn(M)) * ct::umma_yn(M);
+  const int64_t part_floats = std::max<int64_t>((int64_t)d.ksplit * T * mpad,
+                                                d.umma ? (int64_t)d.ksplit_umma * T * ldp_umma : 0);
 #define ALLOC(ptr, n)                    \
   do {                                   \
     int r__ = alloc(s, &(ptr), (n));     \
@@ -612,7 +627,15 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   ALLOC(d.loss_mse_b, d.NB);
   ALLOC(d.loss_mr_b, d.NB);
   ALLOC(d.stepsum_part, T * d.fwd_grid);
-  ALLOC(d.gemm_part, (int64_t)d.ksplit * T * mpad);
+  ALLOC(d.gemm_part, part_floats);
+  if (d.umma) {
+    ALLOC(d.H_hi, B * M * S);
+    ALLOC(d.H_lo, B * M * S);
+    ALLOC(d.Ht_hi, B * S * d.kpad);
+    ALLOC(d.Ht_lo, B * S * d.kpad);
+    ALLOC(d.R_hi, T * d.kpad);
+    ALLOC(d.R_lo, T * d.kpad);
+  }
   ALLOC(d.dmin, 1);
   ALLOC(d.status, 1);
   ALLOC(d.barrier, 1);
@@ -682,6 +705,10 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
     cudaError_t e = ct::launch_min_delay(d, st);
     if (e != cudaSuccess) r = cuda_fail(e, "min delay kernel");
   }
+  if (!r && d.umma) {
+    cudaError_t e = ct::umma_prepare(d, st);
+    if (e != cudaSuccess) r = cuda_fail(e, "tensor-core operand split");
+  }
   if (!r) {
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) r = cuda_fail(e, "scenario upload");
@@ -719,7 +746,10 @@ int ct_scenario_dims(ct_scn* scn, int64_t* S, int64_t* M, int64_t* T, int64_t* B
 int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, int grad_mode, int precision) {
   if (!scn || !batch_index) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
   if (grad_mode != CT_GRAD_REFERENCE) return fail(CT_ERR_NOT_SUPPORTED, "gradient mode %d", grad_mode);
-  if (precision != CT_PREC_FP32) return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
+  if (precision != CT_PREC_FP32 && precision != CT_PREC_TF32X3 && precision != CT_PREC_TF32)
+    return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
+  if (precision != CT_PREC_FP32 && !scn->d.umma)
+    return fail(CT_ERR_NOT_SUPPORTED, "tensor-core precision needs num_states divisible by 4 (16-byte TMA rows)");
   CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
   DeviceScenario& d = scn->d;
   const ct_algorithm& a = scn->algo;
@@ -739,7 +769,7 @@ int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, i
   int64_t batch = 0;
   const bool batched = a.batch_size != 0;
   for (int32_t beat : order) {
-    rc = run_beat(scn, beat);
+    rc = run_beat(scn, beat, precision);
     if (rc) return rc;
     if (batched) {
       batch += 1;

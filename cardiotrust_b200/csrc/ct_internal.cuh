@@ -57,7 +57,14 @@ struct DeviceScenario {
   float* stepsum_part;   // [T, fwd_grid] per-CTA partial max-regularisation sums
   float* gemm_part;      // [ksplit, T, Mpad] split-K partials of H x
   int fwd_grid;          // CTAs of the forward kernel
-  int ksplit;            // split-K factor of the H x product
+  int ksplit;            // split-K factor of the H x product (CUDA-core form)
+  // tensor-core form (ct_umma.cu); null when the scenario does not support it
+  bool umma;             // S % 4 == 0 and the TMA encoder is available
+  int ksplit_umma;       // split-K factor of the tensor-core H x
+  int64_t kpad;          // M rounded up to 32 (K extent of H^T r)
+  float* H_hi, *H_lo;    // [B,M,S] TF32 split of H
+  float* Ht_hi, *Ht_lo;  // [B,S,kpad] TF32 split of H^T, zero padded
+  float* R_hi, *R_lo;    // [T,kpad] TF32 split of the residuals
   int32_t* dmin;         // [1] smallest valid delay
   int32_t* status;       // [1] device-side error code (0 = ok)
   GridBarrier* barrier;  // [1]
@@ -76,6 +83,17 @@ int forward_grid_size(int64_t V, int device);
 cudaError_t launch_measure(DeviceScenario& d, int64_t beat, bool with_residuals, cudaStream_t stream);
 // MR[t,:] = H[beat]^T R[t,:] for all steps.
 cudaError_t launch_map_residuals(DeviceScenario& d, int64_t beat, cudaStream_t stream);
+// loss_mse[t] from R.
+cudaError_t launch_mse(DeviceScenario& d, cudaStream_t stream);
+
+// Tensor-core (tcgen05) forms, ct_umma.cu.
+bool umma_supported(int64_t S, int64_t M);
+int umma_yn(int64_t M);
+int umma_ksplit(int64_t T, int64_t S, int64_t M, int sms);
+cudaError_t umma_prepare(DeviceScenario& d, cudaStream_t stream);
+cudaError_t launch_measure_umma(DeviceScenario& d, int64_t beat, bool with_residuals, int precision,
+                                cudaStream_t stream);
+cudaError_t launch_map_residuals_umma(DeviceScenario& d, int64_t beat, int precision, cudaStream_t stream);
 
 struct DeriveScalars {
   float mse_scaling, reg_scaling, threshold, diffreg;

@@ -133,7 +133,11 @@ cudaError_t launch_measure(DeviceScenario& d, int64_t beat, bool with_residuals,
       with_residuals ? d.R : nullptr);
   err = cudaGetLastError();
   if (err != cudaSuccess || !with_residuals) return err;
-  mse_kernel<<<(unsigned)((T + 127) / 128), 128, 0, stream>>>(d.R, T, M, d.loss_mse);
+  return launch_mse(d, stream);
+}
+
+cudaError_t launch_mse(DeviceScenario& d, cudaStream_t stream) {
+  mse_kernel<<<(unsigned)((d.T + 127) / 128), 128, 0, stream>>>(d.R, d.T, d.M, d.loss_mse);
   return cudaGetLastError();
 }
 

@@ -55,7 +55,11 @@ enum ct_grad_mode {
   CT_GRAD_REFERENCE = 0 /* the reference's per-step derivation, derivation.rs:173-229 */
 };
 /* Arithmetic of the two measurement products (H x and H^T r). */
-enum ct_precision { CT_PREC_FP32 = 0 };
+enum ct_precision {
+  CT_PREC_FP32 = 0,   /* FP32 CUDA-core GEMMs */
+  CT_PREC_TF32X3 = 1, /* tcgen05 TF32 with a hi/lo split of both operands (hi*hi + hi*lo + lo*hi), FP32 accumulate */
+  CT_PREC_TF32 = 2    /* tcgen05 TF32, one pass (operands rounded to TF32) */
+};
 
 /* The Algorithm fields the epoch reads, src/core/config/algorithm.rs:25-58. */
 typedef struct ct_algorithm {

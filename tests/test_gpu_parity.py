@@ -285,3 +285,54 @@ def test_reference_shaped_api(alg, ctx, oracle_mod, cuboid8):
     assert bi.value == 3
     assert lb[0] > lb[1] > lb[2], lb
     eng.close()
+
+
+@pytest.mark.parametrize("precision,tol_meas,tol_grad", [(1, TOL_MEAS, TOL_GRAD), (2, 5e-4, 5e-3)])
+def test_tensor_core_precisions(alg, ctx, oracle_mod, cuboid8, precision, tol_meas, tol_grad):
+    """tcgen05 measurement products: split TF32 keeps the FP32 bars; one-pass TF32 has looser,
+    stated bars (operands rounded to 10-bit mantissas)."""
+    a, oa = algo_pair(alg, oracle_mod, optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
+    eng = alg.EpochEngine.from_scenario(ctx, cuboid8, num_batch_slots=2, algorithm=a)
+    o = oracle_mod.from_scenario(cuboid8, num_batch_slots=2)
+    o64 = oracle_mod.from_scenario(cuboid8, num_batch_slots=2, dtype=np.float64)
+    g0 = cuboid8.model.gains.astype(np.float64)
+    for epoch in range(2):
+        eng.run_epoch(epoch, precision=alg.Precision(precision))
+        o.run_epoch(oa)
+        o64.run_epoch(oa)
+        if epoch == 0:
+            assert_bitwise(eng.read("system_states"), o.system_states, "system_states")
+        assert rel_err(eng.read("measurements"), o64.measurements) < tol_meas * (1 if epoch == 0 else 10)
+        assert rel_err(eng.read("grad_gains"), o64.d_gains) < tol_grad
+        assert rel_err(eng.read("grad_coefs"), o64.d_coefs) < tol_grad
+        assert rel_err(eng.read("gains") - g0, o64.gains - g0) < tol_grad
+        assert rel_err(eng.read("loss_batch"), o64.loss_batch) < 10 * TOL_LOSS
+    eng.close()
+
+
+def test_tensor_core_shapes(alg, ctx, oracle_mod):
+    """tcgen05 path on ragged shapes: T not a multiple of 128, more than 128 sensor rows (two N tiles of
+    the H x product), states not a multiple of the 256-wide H^T r tile."""
+    from cardiotrust_b200 import scenario as sc
+
+    spec = sc.ScenarioSpec(shape=(6, 5, 4), num_steps=203, num_sensors=50, patho_size=2, patho_origin=(2, 2, 1),
+                           pulse_onset=1, pulse_sigma_samples=4.0, noise_fraction=0.01, seed=9)
+    scn = sc.attach_measurements(sc.build(spec), oracle_forward(oracle_mod))
+    assert scn.num_sensors == 150 and scn.num_states % 4 == 0
+    a, oa = algo_pair(alg, oracle_mod, learning_rate=0.5, freeze_delays=False)
+    o64 = oracle_mod.from_scenario(scn, dtype=np.float64)
+    o64.run_epoch(oa)
+    for precision in (alg.Precision.Fp32, alg.Precision.Tf32x3):
+        eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=a)
+        eng.run_epoch(0, precision=precision)
+        assert rel_err(eng.read("measurements"), o64.measurements) < TOL_MEAS, precision
+        assert rel_err(eng.read("mapped_residuals_history"), _mr_history(o64, scn)) < 1e-4, precision
+        assert rel_err(eng.read("grad_gains"), o64.d_gains) < TOL_GRAD, precision
+        eng.close()
+
+
+def _mr_history(o64, scn):
+    """H^T r of every step of the last beat, in float64, from the oracle's residuals."""
+    H = scn.measurement_matrix[-1].astype(np.float64)
+    r = o64.measurements[-1].astype(np.float64) - scn.measurements[-1].astype(np.float64)
+    return r @ H
