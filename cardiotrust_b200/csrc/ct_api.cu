@@ -346,6 +346,47 @@ void scatter_state_columns(float* dst, const float* src, const std::vector<int32
   }
 }
 
+// Per forward tile (kFwdTileVoxels consecutive device voxels): the sorted device voxels its
+// (voxel, offset) items read, and each item's slot in that list. False if a neighbourhood
+// exceeds kFwdHaloMax (the resident forward form is then not used).
+bool build_halos(const ct_scn* s, const std::vector<int32_t>& nbr_ref, int64_t tiles, std::vector<int32_t>& halo,
+                 std::vector<int32_t>& nhalo, std::vector<int16_t>& hslot) {
+  const int TV = ct::kFwdTileVoxels, HM = ct::kFwdHaloMax;
+  const int64_t V = (int64_t)s->perm.size();
+  halo.assign((size_t)(tiles * HM), -1);
+  nhalo.assign((size_t)tiles, 0);
+  hslot.assign((size_t)(tiles * TV * kOffsets), -1);
+  std::vector<int32_t> list;
+  for (int64_t t = 0; t < tiles; ++t) {
+    list.clear();
+    for (int vl = 0; vl < TV; ++vl) {
+      const int64_t u = t * TV + vl;
+      if (u >= V) break;
+      for (int n = 0; n < kOffsets; ++n) {
+        const int32_t w = nbr_ref[(size_t)s->perm[(size_t)u] * kOffsets + n];
+        if (w >= 0) list.push_back(s->inv[(size_t)w]);
+      }
+    }
+    std::sort(list.begin(), list.end());
+    list.erase(std::unique(list.begin(), list.end()), list.end());
+    if ((int)list.size() > HM) return false;
+    nhalo[(size_t)t] = (int32_t)list.size();
+    std::copy(list.begin(), list.end(), halo.begin() + (size_t)(t * HM));
+    for (int vl = 0; vl < TV; ++vl) {
+      const int64_t u = t * TV + vl;
+      if (u >= V) break;
+      for (int n = 0; n < kOffsets; ++n) {
+        const int32_t w = nbr_ref[(size_t)s->perm[(size_t)u] * kOffsets + n];
+        if (w < 0) continue;
+        const int32_t dw = s->inv[(size_t)w];
+        hslot[(size_t)((t * TV + vl) * kOffsets + n)] =
+            (int16_t)(std::lower_bound(list.begin(), list.end(), dw) - list.begin());
+      }
+    }
+  }
+  return true;
+}
+
 int validate_and_build_nbr(const ct_scenario_desc* desc, std::vector<int32_t>& nbr) {
   const int64_t S = desc->num_states, V = S / 3;
   nbr.assign((size_t)(V * kOffsets), -1);
@@ -572,7 +613,14 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   d.T = T;
   d.B = B;
   d.NB = desc->num_batch_slots;
-  d.fwd_grid = ct::forward_grid_size(d.V, ctx->device);
+  // forward form: resident (one tile per CTA, halo ring) when every tile fits a co-resident CTA
+  // and every tile's neighbourhood fits the ring; streaming otherwise
+  const int64_t tiles = (d.V + ct::kFwdTileVoxels - 1) / ct::kFwdTileVoxels;
+  std::vector<int32_t> h_halo, h_nhalo;
+  std::vector<int16_t> h_hslot;
+  d.fwd_ring = tiles <= ct::forward_ring_capacity(ctx->device) &&
+               build_halos(s, nbr, tiles, h_halo, h_nhalo, h_hslot);
+  d.fwd_grid = d.fwd_ring ? (int)tiles : ct::forward_grid_size(d.V, ctx->device);
   {
     const int64_t tiles = ((M + 63) / 64) * ((T + 63) / 64);
     int64_t ks = (2 * ctx->num_sms + tiles - 1) / tiles;
@@ -636,7 +684,12 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
     ALLOC(d.R_hi, T * d.kpad);
     ALLOC(d.R_lo, T * d.kpad);
   }
-  ALLOC(d.dmin, 1);
+  ALLOC(d.dmin, 2);
+  if (d.fwd_ring) {
+    ALLOC(d.halo, tiles * ct::kFwdHaloMax);
+    ALLOC(d.hslot, tiles * ct::kFwdTileVoxels * kOffsets);
+    ALLOC(d.nhalo, tiles);
+  }
   ALLOC(d.status, 1);
   ALLOC(d.barrier, 1);
 #undef ALLOC
@@ -665,6 +718,11 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   r = r ? r : upload(s, d.init_delays, h_init.data(), sizeof(float) * V * kOffsets);
   r = r ? r : upload(s, d.H, h_H.data(), sizeof(float) * B * M * S);
   r = r ? r : upload(s, d.ctrl, h_ctrl.data(), sizeof(float) * S);
+  if (d.fwd_ring) {
+    r = r ? r : upload(s, d.halo, h_halo.data(), sizeof(int32_t) * h_halo.size());
+    r = r ? r : upload(s, d.hslot, h_hslot.data(), sizeof(int16_t) * h_hslot.size());
+    r = r ? r : upload(s, d.nhalo, h_nhalo.data(), sizeof(int32_t) * h_nhalo.size());
+  }
   r = r ? r : upload(s, d.u, desc->control_function, sizeof(float) * T);
   if (!r && desc->measurements) r = upload(s, d.meas, desc->measurements, sizeof(float) * B * T * M);
   if (!r && !desc->measurements) {

@@ -11,14 +11,13 @@ namespace ct {
 constexpr int kOffsets = 26;   // neighbour offsets per voxel
 constexpr int kGainCols = 78;  // 26 offsets x 3 neighbour components
 constexpr int kMaxStepBlock = 8;  // steps advanced between grid barriers in the forward kernel
+constexpr int kFwdTileVoxels = 32;  // voxels per forward tile (consecutive in device order)
+constexpr int kFwdHaloMax = 160;    // largest neighbourhood of a tile the resident forward form stages
 
-// Spin limit of every device-side wait (~1 s of polling with a 64 ns back-off).
-constexpr long long kSpinLimit = 1ll << 24;
-
-// Device-side grid barrier state (generation counting).
+// Device-side grid barrier state: a monotone arrival counter, zeroed before each launch.
 struct GridBarrier {
   unsigned int count;
-  unsigned int generation;
+  unsigned int unused;
 };
 
 // Everything of one scenario that lives on the device.
@@ -65,7 +64,12 @@ struct DeviceScenario {
   float* H_hi, *H_lo;    // [B,M,S] TF32 split of H
   float* Ht_hi, *Ht_lo;  // [B,S,kpad] TF32 split of H^T, zero padded
   float* R_hi, *R_lo;    // [T,kpad] TF32 split of the residuals
-  int32_t* dmin;         // [1] smallest valid delay
+  int32_t* dmin;         // [2] smallest and largest delay of a connected (voxel, offset) pair
+  // resident forward form (one tile per CTA, halo history in a shared ring)
+  bool fwd_ring;
+  int32_t* halo;         // [tiles, kFwdHaloMax] device voxels of each tile's neighbourhood
+  int16_t* hslot;        // [tiles, 26 * kFwdTileVoxels] halo slot of each item's neighbour, -1 if absent
+  int32_t* nhalo;        // [tiles]
   int32_t* status;       // [1] device-side error code (0 = ok)
   GridBarrier* barrier;  // [1]
 };
@@ -77,7 +81,9 @@ int report_error(int status, const char* message);
 
 // Forward propagation of one beat: X[t,:] for t in [0,T).
 cudaError_t launch_forward(DeviceScenario& d, float threshold, cudaStream_t stream);
+// CTAs of the streaming form, and how many CTAs of the resident form fit on the device.
 int forward_grid_size(int64_t V, int device);
+int forward_ring_capacity(int device);
 
 // y = H[beat] x for all steps; Y[beat] = y, R = y - meas[beat], loss_mse[t].
 cudaError_t launch_measure(DeviceScenario& d, int64_t beat, bool with_residuals, cudaStream_t stream);

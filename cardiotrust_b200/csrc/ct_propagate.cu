@@ -14,20 +14,25 @@
 //   * Every read of the recurrence is of x[t-d] or x[t-d-1] with d >= 1, so
 //     the states of steps t .. t+L-1 are independent when L <= min delay.
 //     The kernel advances L = min(dmin, kMaxStepBlock) steps between two grid
-//     barriers.
+//     barriers (monotone counter, ct_sync.cuh).
 //   * The all-pass state is deduplicated: ap_outputs[3v+a, 3n+b] does not
 //     depend on the row component a (same input state, coefficient and zero
 //     start, prediction.rs:56-79), so it is kept as [V, 26*3].
-//   * Shared memory holds, per tile: the gains transposed to [k][state]
-//     (entries of absent neighbours zeroed, which adds exact zeros where the
-//     reference skips), the (neighbour, delay, coefficient) of each
-//     (voxel, offset) pair, the all-pass state, and the all-pass outputs of
-//     one round of steps. A CTA that owns one tile stages it once per launch.
-//   * A block of L steps runs in rounds of kSlots steps. Phase A: one thread
-//     per (voxel, offset) runs the three all-pass chains for the round's steps;
-//     its 3 (kSlots + 1) history loads are independent and issued together.
-//     Phase B: one thread per (voxel, row component, step parity) sums the 78
-//     gain-weighted outputs in column order k = 0..77 for its steps.
+//   * Warp specialisation. A block of L steps runs as rounds of kRound steps
+//     through a double-buffered ring of all-pass outputs in shared memory.
+//     Producer warps: one thread per (voxel, offset) runs the three all-pass
+//     chains of the round; its 3 (kRound + 1) history loads are independent.
+//     Consumer warps: one thread per (voxel, step) accumulates the three rows
+//     x[t, 3v+a] over the 78 columns in order k = 0..77 (float2 all-pass and
+//     float4 gain loads feed three independent chains), adds the control
+//     input, stores the states and the voxel's max-regularisation term.
+//     Named barriers hand the two buffers back and forth; no CTA-wide barrier
+//     separates the roles inside a block.
+//   * Shared memory per tile: gains as float4 {g[3v][k], g[3v+1][k],
+//     g[3v+2][k], 0} (absent neighbours zeroed, which adds exact zeros where
+//     the reference skips), (neighbour, delay, coefficient) per (voxel,
+//     offset), the chain state, and the two round buffers. A CTA that owns one
+//     tile stages it once per launch.
 //   * History reads go through L1: within one launch a history row is read
 //     only after the grid barrier that completes it, so no SM can hold a
 //     stale line of it (L1 holds no global data across launches).
@@ -39,13 +44,15 @@
 namespace ct {
 namespace {
 
-constexpr int kTileVoxels = 32;
+constexpr int kTileVoxels = kFwdTileVoxels;
 constexpr int kTileStates = 3 * kTileVoxels;
 constexpr int kTileItems = kTileVoxels * kOffsets;  // (voxel, offset) pairs
-constexpr int kThreads = 256;
-constexpr int kParity = 2;  // phase-B step groups per state
-constexpr int kItemsPerThread = (kTileItems + kThreads - 1) / kThreads;
-constexpr int kSlots = 4;   // steps per round: a block of L steps runs in ceil(L / kSlots) rounds
+constexpr int kRound = 2;                            // steps per round
+constexpr int kProducers = 128;                      // 4 warps
+constexpr int kConsumers = kRound * kTileVoxels;     // 2 warps: (step, voxel)
+constexpr int kThreads = kProducers + kConsumers;
+constexpr int kBarFull = 1;   // named barriers kBarFull + buffer, kBarEmpty + buffer
+constexpr int kBarEmpty = 3;
 
 struct FwdArgs {
   int V, S, T;
@@ -66,44 +73,52 @@ struct FwdArgs {
 };
 
 struct Smem {
-  float gT[kGainCols][kTileStates];           // gains, transposed, absent neighbours zeroed
-  float ap_out[kSlots][kTileVoxels * kGainCols];
+  float4 g[kGainCols][kTileVoxels];                  // gains of the voxel's three rows at column k
+  float ap_out[2][kRound][kTileVoxels * kGainCols];  // round buffers
   float ap_state[kTileVoxels * kGainCols];
-  float x[kMaxStepBlock][kTileStates];
-  int32_t j[kTileItems];                       // 3 * neighbour, -1 if absent
+  int32_t j[kTileItems];                             // 3 * neighbour, -1 if absent
   int32_t d[kTileItems];
   float c[kTileItems];
   float ctrl[kTileStates];
   float part[kMaxStepBlock];
 };
 
-// Stage one tile: metadata first (the gain mask needs it), then the gains and the chain state.
+__device__ __forceinline__ void named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id, int count) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Stage one tile (all threads): metadata first (the gain mask needs it), then gains and chain state.
 __device__ __forceinline__ void stage_tile(Smem& sm, const FwdArgs& p, int v0) {
   const int nv = min(kTileVoxels, p.V - v0);
   for (int e = threadIdx.x; e < kTileItems; e += blockDim.x) {
     const int vl = e / kOffsets;
     if (vl < nv) {
-      const int g = v0 * kOffsets + e;
-      const int32_t nb = p.nbr[g];
+      const int gi = v0 * kOffsets + e;
+      const int32_t nb = p.nbr[gi];
       sm.j[e] = nb < 0 ? -1 : 3 * nb;
-      sm.d[e] = p.delays[g];
-      sm.c[e] = p.coefs[g];
+      sm.d[e] = p.delays[gi];
+      sm.c[e] = p.coefs[gi];
     } else {
       sm.j[e] = -1;
       sm.d[e] = 1;
       sm.c[e] = 0.0f;
     }
   }
-  for (int e = threadIdx.x; e < kTileStates; e += blockDim.x)
-    sm.ctrl[e] = (e < 3 * nv) ? p.ctrl[3 * v0 + e] : 0.0f;
+  for (int e = threadIdx.x; e < kTileStates; e += blockDim.x) sm.ctrl[e] = (e < 3 * nv) ? p.ctrl[3 * v0 + e] : 0.0f;
   __syncthreads();
-  // gains: coalesced along each row, written transposed
-  const float* g0 = p.gains + (size_t)3 * v0 * kGainCols;
-  for (int e = threadIdx.x; e < kTileStates * kGainCols; e += blockDim.x) {
-    const int st = e / kGainCols, k = e - st * kGainCols;
-    float g = 0.0f;
-    if (st < 3 * nv && sm.j[(st / 3) * kOffsets + k / 3] >= 0) g = g0[e];
-    sm.gT[k][st] = g;
+  for (int e = threadIdx.x; e < kGainCols * kTileVoxels; e += blockDim.x) {
+    const int k = e / kTileVoxels, vl = e - k * kTileVoxels;
+    float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (vl < nv && sm.j[vl * kOffsets + k / 3] >= 0) {
+      const float* row = p.gains + (size_t)3 * (v0 + vl) * kGainCols + k;
+      g.x = row[0];
+      g.y = row[kGainCols];
+      g.z = row[2 * kGainCols];
+    }
+    sm.g[k][vl] = g;
   }
   const float* a0 = p.ap + (size_t)v0 * kGainCols;
   for (int e = threadIdx.x; e < kTileVoxels * kGainCols; e += blockDim.x)
@@ -117,122 +132,391 @@ __device__ __forceinline__ void unstage_tile(Smem& sm, const FwdArgs& p, int v0)
   for (int e = threadIdx.x; e < nv * kGainCols; e += blockDim.x) a0[e] = sm.ap_state[e];
 }
 
-__global__ void __launch_bounds__(kThreads, 1) forward_kernel(FwdArgs p) {
+// Producer: all-pass chains of steps tr0 .. tr0+R-1 into round buffer `buf`. Each thread owns
+// up to kItemsPerProducer (voxel, offset) items and issues the history loads of all of them
+// before any chain arithmetic, so ~60 independent loads are in flight per thread.
+constexpr int kItemsPerProducer = (kTileItems + kProducers - 1) / kProducers;
+
+__device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int nv, int tr0, int R, int buf) {
+  // h[i][q][b] = x[tr0 - d_i - 1 + q, j_i + b]: in(tr0+s) = h[s+1], in_delayed(tr0+s) = h[s];
+  // rows before t = 0 read as zero (prediction.rs:68-77)
+  float h[kItemsPerProducer][kRound + 1][3];
+#pragma unroll
+  for (int i = 0; i < kItemsPerProducer; ++i) {
+    const int e = threadIdx.x + i * kProducers;
+    const int jb = e < kTileItems ? sm.j[e] : -1;
+    const int d = e < kTileItems ? sm.d[e] : 0;
+#pragma unroll
+    for (int q = 0; q <= kRound; ++q) {
+      const int tr = tr0 - d - 1 + q;
+      const bool ok = jb >= 0 && q <= R && tr >= 0;
+      const float* row = p.X + (size_t)(ok ? tr : 0) * p.S + (jb >= 0 ? jb : 0);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) h[i][q][b] = ok ? row[b] : 0.0f;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < kItemsPerProducer; ++i) {
+    const int e = threadIdx.x + i * kProducers;
+    if (e >= kTileItems) break;
+    const int vl = e / kOffsets;
+    const int n = e - vl * kOffsets;
+    const int jb = sm.j[e];
+    float* st = sm.ap_state + vl * kGainCols + 3 * n;
+    float* out0 = sm.ap_out[buf][0] + vl * kGainCols + 3 * n;
+    if (jb >= 0) {
+      const float c = sm.c[e];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        float a = st[b];
+#pragma unroll
+        for (int s = 0; s < kRound; ++s) {
+          if (s < R) {
+            a = fmaf(c, h[i][s + 1][b] - a, h[i][s][b]);
+            out0[s * (kTileVoxels * kGainCols) + b] = a;
+            if (tr0 + s == p.T - 2) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = a;
+          }
+        }
+        st[b] = a;
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < kRound; ++s)
+        if (s < R)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) out0[s * (kTileVoxels * kGainCols) + b] = 0.0f;
+      if (vl < nv && p.T - 2 >= tr0 && p.T - 2 < tr0 + R)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = st[b];
+    }
+  }
+}
+
+// Consumer: states of step tr0 + s for voxel vl (thread = (s, vl)), and the voxel's
+// max-regularisation term reduced over the warp (the warp covers one step).
+__device__ __forceinline__ void consume(Smem& sm, const FwdArgs& p, int v0, int nv, int tr0, int R, int buf,
+                                       int r0) {
+  const int ct = threadIdx.x - kProducers;
+  const int s = ct / kTileVoxels, vl = ct - s * kTileVoxels;
+  if (s >= R) return;  // warp-uniform
+  float f2 = 0.0f;
+  if (vl < nv) {
+    const float* aps = sm.ap_out[buf][s] + vl * kGainCols;
+    float x0 = 0.0f, x1 = 0.0f, x2 = 0.0f;
+#pragma unroll 3
+    for (int k = 0; k < kGainCols; k += 2) {
+      const float2 a = *reinterpret_cast<const float2*>(aps + k);
+      const float4 g0 = sm.g[k][vl];
+      const float4 g1 = sm.g[k + 1][vl];
+      x0 = x0 + g0.x * a.x;
+      x1 = x1 + g0.y * a.x;
+      x2 = x2 + g0.z * a.x;
+      x0 = x0 + g1.x * a.y;
+      x1 = x1 + g1.y * a.y;
+      x2 = x2 + g1.z * a.y;
+    }
+    const int t = tr0 + s;
+    const float uc = p.u[t];
+    x0 = x0 + uc * sm.ctrl[3 * vl];
+    x1 = x1 + uc * sm.ctrl[3 * vl + 1];
+    x2 = x2 + uc * sm.ctrl[3 * vl + 2];
+    float* xo = p.X + (size_t)t * p.S + 3 * (v0 + vl);
+    xo[0] = x0;
+    xo[1] = x1;
+    xo[2] = x2;
+    const float sum = fabsf(x0) + fabsf(x1) + fabsf(x2);
+    if (sum > p.threshold) {
+      const float f = sum - p.threshold;
+      f2 = f * f;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) f2 = f2 + __shfl_down_sync(0xffffffffu, f2, off);
+  if (vl == 0) sm.part[r0 + s] = sm.part[r0 + s] + f2;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) forward_stream_kernel(FwdArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
 
-  const int V = p.V, S = p.S, T = p.T;
+  const int V = p.V, T = p.T;
   const int num_tiles = (V + kTileVoxels - 1) / kTileVoxels;
   const bool resident = num_tiles <= (int)gridDim.x;  // this CTA owns at most one tile
-  int dmin = *p.dmin;
+  const bool producer = threadIdx.x < kProducers;
+  int dmin = p.dmin[0];
   if (dmin < 1) dmin = 1;
   const int Lmax = dmin < kMaxStepBlock ? dmin : kMaxStepBlock;
 
   if (resident && (int)blockIdx.x < num_tiles) stage_tile(sm, p, blockIdx.x * kTileVoxels);
 
+  int round = 0;  // rounds issued by this CTA, pairs the named barriers across blocks and tiles
+  unsigned int barrier_number = 0;
   for (int t0 = 0; t0 < T; t0 += Lmax) {
     const int L = (T - t0) < Lmax ? (T - t0) : Lmax;
     if (threadIdx.x < kMaxStepBlock) sm.part[threadIdx.x] = 0.0f;
+    __syncthreads();
 
     for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
       const int v0 = tile * kTileVoxels;
       const int nv = min(kTileVoxels, V - v0);
       if (!resident) stage_tile(sm, p, v0);
+      for (int r0 = 0; r0 < L; r0 += kRound, ++round) {
+        const int R = (L - r0) < kRound ? (L - r0) : kRound;
+        const int buf = round & 1;
+        if (producer) {
+          if (round >= 2) named_sync(kBarEmpty + buf, kThreads);
+          produce(sm, p, v0, nv, t0 + r0, R, buf);
+          named_arrive(kBarFull + buf, kThreads);
+        } else {
+          named_sync(kBarFull + buf, kThreads);
+          consume(sm, p, v0, nv, t0 + r0, R, buf, r0);
+          named_arrive(kBarEmpty + buf, kThreads);
+        }
+      }
+      if (!resident) {
+        __syncthreads();
+        unstage_tile(sm, p, v0);
+      }
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < L) p.stepsum_part[(size_t)(t0 + threadIdx.x) * gridDim.x + blockIdx.x] = sm.part[threadIdx.x];
+    if (t0 + L < T) {
+      if (!grid_barrier(p.barrier, barrier_number++, p.status)) return;
+    }
+  }
+  if (resident && (int)blockIdx.x < num_tiles) {
+    __syncthreads();
+    unstage_tile(sm, p, blockIdx.x * kTileVoxels);
+  }
+}
 
-      for (int r0 = 0; r0 < L; r0 += kSlots) {
-        const int R = (L - r0) < kSlots ? (L - r0) : kSlots;  // steps in this round
-        const int tr0 = t0 + r0;                                // first step of the round
-        // ---- phase A: three all-pass chains per (voxel, offset)
+
+// ---- resident form: one tile per CTA for the whole launch, neighbour history in a shared ring
+//
+// Each tile's halo (the device voxels its 26-neighbourhoods touch, at most
+// kHaloMax) is listed on the host; producer thread p owns the items
+// e = p + kProducers * i and keeps their halo slot, delay, coefficient and
+// three chain states in registers for the whole launch. History rows live
+// in a ring of kRingRows rows x halo states in shared memory: each round
+// needs rows [t - dmax - 1, t + kRound - 1 - dmin], stages the rows new to
+// the window with cp.async one round ahead (the first round of a block
+// stages after the grid barrier, since its rows were produced in the
+// previous block), and the chains read only shared memory. When the spread
+// of delays does not fit the ring, the producers read the history from
+// global memory instead (same arithmetic, same results).
+
+constexpr int kHaloMax = kFwdHaloMax;
+constexpr int kRingRows = 16;  // power of two: slot = row & (kRingRows - 1)
+constexpr int kBarProducers = 5;
+
+struct RingSmem {
+  float4 g[kGainCols][kTileVoxels];
+  float ap_out[2][kRound][kTileVoxels * kGainCols];
+  float ring[kRingRows][kHaloMax * 3];
+  int32_t halo[kHaloMax];  // device voxel of each halo slot
+  float ctrl[kTileStates];
+  float part[kMaxStepBlock];
+};
+
+struct RingArgs {
+  const int32_t* halo;    // [tiles, kHaloMax], -1 padded
+  const int16_t* hslot;   // [tiles, kTileItems], halo slot of the item's neighbour, -1 if absent
+  const int32_t* nhalo;   // [tiles]
+};
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// Producers: copy history rows [r_lo, r_hi] of the halo into the ring (rows before t = 0 are zero).
+__device__ __forceinline__ void stage_rows(RingSmem& sm, const FwdArgs& p, int nh, int r_lo, int r_hi) {
+  const int per_row = 3 * nh;
+  const int total = (r_hi - r_lo + 1) * per_row;
+  for (int f = threadIdx.x; f < total; f += kProducers) {
+    const int rr = f / per_row, rem = f - rr * per_row;
+    const int row = r_lo + rr;
+    float* dst = &sm.ring[row & (kRingRows - 1)][rem];
+    if (row < 0) {
+      *dst = 0.0f;
+    } else {
+      const int hv = rem / 3, b = rem - 3 * (rem / 3);
+      cp_async4(dst, p.X + (size_t)row * p.S + 3 * sm.halo[hv] + b);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) forward_ring_kernel(FwdArgs p, RingArgs ra) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RingSmem& sm = *reinterpret_cast<RingSmem*>(smem_raw);
+  const int T = p.T, S = p.S;
+  const int tile = blockIdx.x;
+  const int v0 = tile * kTileVoxels;
+  const int nv = min(kTileVoxels, p.V - v0);
+  const int nh = ra.nhalo[tile];
+  const bool producer = threadIdx.x < kProducers;
+  int dmin = p.dmin[0], dmax = p.dmin[1];
+  if (dmin < 1) dmin = 1;
+  if (dmax < dmin) dmax = dmin;
+  const int Lmax = dmin < kMaxStepBlock ? dmin : kMaxStepBlock;
+  // rows a round reads: [tr0 - dmax - 1, tr0 + kRound - 1 - dmin]; plus kRound rows staged ahead
+  const bool use_ring = (dmax - dmin + kRound + 1) + kRound <= kRingRows;
+
+  // ---- set-up: gains (transposed, masked), control, halo list, zeroed ring
+  for (int e = threadIdx.x; e < kGainCols * kTileVoxels; e += blockDim.x) {
+    const int k = e / kTileVoxels, vl = e - k * kTileVoxels;
+    float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (vl < nv && p.nbr[(v0 + vl) * kOffsets + k / 3] >= 0) {
+      const float* row = p.gains + (size_t)3 * (v0 + vl) * kGainCols + k;
+      g.x = row[0];
+      g.y = row[kGainCols];
+      g.z = row[2 * kGainCols];
+    }
+    sm.g[k][vl] = g;
+  }
+  for (int e = threadIdx.x; e < kTileStates; e += blockDim.x) sm.ctrl[e] = (e < 3 * nv) ? p.ctrl[3 * v0 + e] : 0.0f;
+  for (int e = threadIdx.x; e < kHaloMax; e += blockDim.x) sm.halo[e] = e < nh ? ra.halo[tile * kHaloMax + e] : 0;
+  for (int e = threadIdx.x; e < kRingRows * kHaloMax * 3; e += blockDim.x) (&sm.ring[0][0])[e] = 0.0f;
+
+  // producer item registers
+  int hs[kItemsPerProducer], dd[kItemsPerProducer], jj[kItemsPerProducer];
+  float cc[kItemsPerProducer], st[kItemsPerProducer][3];
 #pragma unroll
-        for (int r = 0; r < kItemsPerThread; ++r) {
-          const int e = threadIdx.x + r * kThreads;
+  for (int i = 0; i < kItemsPerProducer; ++i) {
+    const int e = threadIdx.x + i * kProducers;
+    hs[i] = -1;
+    dd[i] = 1;
+    jj[i] = 0;
+    cc[i] = 0.0f;
+    st[i][0] = st[i][1] = st[i][2] = 0.0f;
+    if (producer && e < kTileItems && e / kOffsets < nv) {
+      const int gi = v0 * kOffsets + e;
+      const int32_t nb = p.nbr[gi];
+      if (nb >= 0) {
+        hs[i] = ra.hslot[(size_t)tile * kTileItems + e];
+        dd[i] = p.delays[gi];
+        cc[i] = p.coefs[gi];
+        jj[i] = 3 * nb;
+      }
+    }
+  }
+  __syncthreads();
+
+  int round = 0;
+  unsigned int barrier_number = 0;
+  int staged_top = -dmin - 1 + kRound - 1 - kRound;  // highest ring row staged so far (none)
+
+  for (int t0 = 0; t0 < T; t0 += Lmax) {
+    const int L = (T - t0) < Lmax ? (T - t0) : Lmax;
+    if (threadIdx.x < kMaxStepBlock) sm.part[threadIdx.x] = 0.0f;
+    __syncthreads();
+    for (int r0 = 0; r0 < L; r0 += kRound, ++round) {
+      const int R = (L - r0) < kRound ? (L - r0) : kRound;
+      const int tr0 = t0 + r0;
+      const int buf = round & 1;
+      const int top = tr0 + R - 1 - dmin;  // newest history row this round reads
+      if (producer) {
+        if (use_ring) {
+          if (r0 == 0 && top > staged_top) {  // first round of a block: rows produced in the previous block
+            stage_rows(sm, p, nh, staged_top + 1, top);
+            staged_top = top;
+          }
+          cp_async_commit_wait_all();
+          named_sync(kBarProducers, kProducers);  // ring rows of this round visible to all producers
+          // stage the next round's new rows (all older than t0) while this round computes
+          const int r0n = r0 + kRound;
+          if (r0n < L) {
+            const int Rn = (L - r0n) < kRound ? (L - r0n) : kRound;
+            const int topn = t0 + r0n + Rn - 1 - dmin;
+            if (topn > staged_top) {
+              stage_rows(sm, p, nh, staged_top + 1, topn);
+              staged_top = topn;
+            }
+          }
+          cp_async_commit();
+        }
+        if (round >= 2) named_sync(kBarEmpty + buf, kThreads);
+#pragma unroll
+        for (int i = 0; i < kItemsPerProducer; ++i) {
+          const int e = threadIdx.x + i * kProducers;
           if (e >= kTileItems) break;
           const int vl = e / kOffsets;
           const int n = e - vl * kOffsets;
-          const int jb = sm.j[e];
-          float* st = sm.ap_state + vl * kGainCols + 3 * n;
-          if (jb >= 0) {
-            const int d = sm.d[e];
-            const float c = sm.c[e];
-            // h[q][b] = x[tr0 - d - 1 + q, jb + b]; in(tr0+s) = h[s+1], in_delayed(tr0+s) = h[s];
-            // rows before t = 0 read as zero (prediction.rs:68-77)
-            float h[kSlots + 1][3];
+          float* out0 = sm.ap_out[buf][0] + vl * kGainCols + 3 * n;
+          if (hs[i] >= 0) {
+            float h[kRound + 1][3];
 #pragma unroll
-            for (int q = 0; q <= kSlots; ++q) {
-              const int tr = tr0 - d - 1 + q;
-              const bool ok = q <= R && tr >= 0;
-              const float* row = p.X + (size_t)(ok ? tr : 0) * S + jb;
+            for (int q = 0; q <= kRound; ++q) {
+              const int row = tr0 - dd[i] - 1 + q;
+              const bool ok = q <= R && row >= 0;
+              if (use_ring) {
+                const float* src = &sm.ring[row & (kRingRows - 1)][3 * hs[i]];
 #pragma unroll
-              for (int b = 0; b < 3; ++b) h[q][b] = ok ? row[b] : 0.0f;
+                for (int b = 0; b < 3; ++b) h[q][b] = ok ? src[b] : 0.0f;
+              } else {
+                const float* src = p.X + (size_t)(ok ? row : 0) * S + jj[i];
+#pragma unroll
+                for (int b = 0; b < 3; ++b) h[q][b] = ok ? src[b] : 0.0f;
+              }
             }
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-              float a = st[b];
+              float a = st[i][b];
 #pragma unroll
-              for (int s = 0; s < kSlots; ++s) {
-                if (s < R) {
-                  a = fmaf(c, h[s + 1][b] - a, h[s][b]);
-                  sm.ap_out[s][vl * kGainCols + 3 * n + b] = a;
-                  if (tr0 + s == T - 2) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = a;
+              for (int s2 = 0; s2 < kRound; ++s2) {
+                if (s2 < R) {
+                  a = fmaf(cc[i], h[s2 + 1][b] - a, h[s2][b]);
+                  out0[s2 * (kTileVoxels * kGainCols) + b] = a;
+                  if (tr0 + s2 == T - 2) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = a;
                 }
               }
-              st[b] = a;
+              st[i][b] = a;
             }
           } else {
 #pragma unroll
-            for (int s = 0; s < kSlots; ++s)
-              if (s < R)
+            for (int s2 = 0; s2 < kRound; ++s2)
+              if (s2 < R)
 #pragma unroll
-                for (int b = 0; b < 3; ++b) sm.ap_out[s][vl * kGainCols + 3 * n + b] = 0.0f;
-            if (vl < nv && T - 2 >= tr0 && T - 2 < tr0 + R)
-#pragma unroll
-              for (int b = 0; b < 3; ++b) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = st[b];
+                for (int b = 0; b < 3; ++b) out0[s2 * (kTileVoxels * kGainCols) + b] = 0.0f;
           }
         }
-        __syncthreads();
-
-        // ---- phase B: gain-weighted sums in column order, plus the control input
-        if (threadIdx.x < kTileStates * kParity) {
-          const int par = threadIdx.x / kTileStates;
-          const int st = threadIdx.x - par * kTileStates;
-          const int vl = st / 3;
-          if (vl < nv) {
-            constexpr int Q = kSlots / kParity;
-            float acc[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) acc[q] = 0.0f;
-#pragma unroll 6
-            for (int k = 0; k < kGainCols; ++k) {
-              const float g = sm.gT[k][st];
-#pragma unroll
-              for (int q = 0; q < Q; ++q) {
-                const int s = par + kParity * q;
-                if (s < R) acc[q] = acc[q] + g * sm.ap_out[s][vl * kGainCols + k];
-              }
-            }
-            const float cm = sm.ctrl[st];
-            float* xcol = p.X + 3 * v0 + st;
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-              const int s = par + kParity * q;
-              if (s < R) {
-                const float x = acc[q] + p.u[tr0 + s] * cm;
-                xcol[(size_t)(tr0 + s) * S] = x;
-                sm.x[r0 + s][st] = x;
-              }
-            }
-          }
-        }
-        __syncthreads();
-      }
-
-      // ---- maximum-regularisation contribution of this tile, per step (fixed-order tree)
-      if (threadIdx.x < 32) {
-        const int vl = threadIdx.x;
-        for (int s = 0; s < L; ++s) {
+        named_arrive(kBarFull + buf, kThreads);
+      } else {
+        named_sync(kBarFull + buf, kThreads);
+        // consumers: same arithmetic as the streaming form
+        const int ct = threadIdx.x - kProducers;
+        const int s2 = ct / kTileVoxels, vl = ct - s2 * kTileVoxels;
+        if (s2 < R) {
           float f2 = 0.0f;
           if (vl < nv) {
-            const float sum = fabsf(sm.x[s][3 * vl]) + fabsf(sm.x[s][3 * vl + 1]) + fabsf(sm.x[s][3 * vl + 2]);
+            const float* aps = sm.ap_out[buf][s2] + vl * kGainCols;
+            float x0 = 0.0f, x1 = 0.0f, x2 = 0.0f;
+#pragma unroll 3
+            for (int k = 0; k < kGainCols; k += 2) {
+              const float2 a = *reinterpret_cast<const float2*>(aps + k);
+              const float4 g0 = sm.g[k][vl];
+              const float4 g1 = sm.g[k + 1][vl];
+              x0 = x0 + g0.x * a.x;
+              x1 = x1 + g0.y * a.x;
+              x2 = x2 + g0.z * a.x;
+              x0 = x0 + g1.x * a.y;
+              x1 = x1 + g1.y * a.y;
+              x2 = x2 + g1.z * a.y;
+            }
+            const int t = tr0 + s2;
+            const float uc = p.u[t];
+            x0 = x0 + uc * sm.ctrl[3 * vl];
+            x1 = x1 + uc * sm.ctrl[3 * vl + 1];
+            x2 = x2 + uc * sm.ctrl[3 * vl + 2];
+            float* xo = p.X + (size_t)t * S + 3 * (v0 + vl);
+            xo[0] = x0;
+            xo[1] = x1;
+            xo[2] = x2;
+            const float sum = fabsf(x0) + fabsf(x1) + fabsf(x2);
             if (sum > p.threshold) {
               const float f = sum - p.threshold;
               f2 = f * f;
@@ -240,40 +524,57 @@ __global__ void __launch_bounds__(kThreads, 1) forward_kernel(FwdArgs p) {
           }
 #pragma unroll
           for (int off = 16; off > 0; off >>= 1) f2 = f2 + __shfl_down_sync(0xffffffffu, f2, off);
-          if (vl == 0) sm.part[s] = sm.part[s] + f2;
+          if (vl == 0) sm.part[r0 + s2] = sm.part[r0 + s2] + f2;
         }
+        named_arrive(kBarEmpty + buf, kThreads);
       }
-      if (!resident) {
-        __syncthreads();
-        unstage_tile(sm, p, v0);
-      }
-      __syncthreads();
     }
+    __syncthreads();
     if ((int)threadIdx.x < L) p.stepsum_part[(size_t)(t0 + threadIdx.x) * gridDim.x + blockIdx.x] = sm.part[threadIdx.x];
     if (t0 + L < T) {
-      if (!grid_barrier(p.barrier, p.status)) return;
+      if (!grid_barrier(p.barrier, barrier_number++, p.status)) {
+        if (producer) cp_async_commit_wait_all();
+        return;
+      }
     }
   }
-  if (resident && (int)blockIdx.x < num_tiles) unstage_tile(sm, p, blockIdx.x * kTileVoxels);
+  if (producer) {
+    cp_async_commit_wait_all();
+#pragma unroll
+    for (int i = 0; i < kItemsPerProducer; ++i) {
+      const int e = threadIdx.x + i * kProducers;
+      if (e < kTileItems && e / kOffsets < nv)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) p.ap[(size_t)v0 * kGainCols + 3 * e + b] = st[i][b];
+    }
+  }
 }
-
 }  // namespace
 
 int forward_grid_size(int64_t V, int device) {
   static bool configured[128] = {};
   if (device >= 0 && device < 128 && !configured[device]) {
-    cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+    cudaFuncSetAttribute(forward_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+    cudaFuncSetAttribute(forward_ring_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RingSmem));
     configured[device] = true;
   }
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, forward_kernel, kThreads, sizeof(Smem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, forward_stream_kernel, kThreads, sizeof(Smem));
   if (per_sm < 1) per_sm = 1;
   const int64_t tiles = (V + kTileVoxels - 1) / kTileVoxels;
   int64_t grid = (int64_t)sms * per_sm;
   if (tiles < grid) grid = tiles;
   if (grid < 1) grid = 1;
   return (int)grid;
+}
+
+int forward_ring_capacity(int device) {
+  forward_grid_size(1, device);  // sets the shared-memory attributes
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, forward_ring_kernel, kThreads, sizeof(RingSmem));
+  return sms * per_sm;
 }
 
 cudaError_t launch_forward(DeviceScenario& d, float threshold, cudaStream_t stream) {
@@ -301,9 +602,19 @@ cudaError_t launch_forward(DeviceScenario& d, float threshold, cudaStream_t stre
   if (err != cudaSuccess) return err;
   err = cudaMemsetAsync(d.barrier, 0, sizeof(GridBarrier), stream);
   if (err != cudaSuccess) return err;
+  if (d.fwd_ring) {
+    RingArgs r;
+    r.halo = d.halo;
+    r.hslot = d.hslot;
+    r.nhalo = d.nhalo;
+    void* args[] = {&a, &r};
+    return cudaLaunchCooperativeKernel((const void*)forward_ring_kernel, dim3(d.fwd_grid), dim3(kThreads), args,
+                                       sizeof(RingSmem), stream);
+  }
   void* args[] = {&a};
-  return cudaLaunchCooperativeKernel((const void*)forward_kernel, dim3(d.fwd_grid), dim3(kThreads), args,
+  return cudaLaunchCooperativeKernel((const void*)forward_stream_kernel, dim3(d.fwd_grid), dim3(kThreads), args,
                                      sizeof(Smem), stream);
 }
 
 }  // namespace ct
+

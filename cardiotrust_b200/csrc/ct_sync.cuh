@@ -5,39 +5,51 @@
 
 namespace ct {
 
-// Grid-wide barrier for a cooperative launch (all CTAs co-resident).
-// Every wait is bounded: after kSpinLimit polls the CTA records CT_ERR_TIMEOUT
-// in *status and returns false; CTAs also leave early once another CTA has
-// recorded an error. Callers must stop issuing work when this returns false.
-__device__ __forceinline__ bool grid_barrier(GridBarrier* bar, int32_t* status) {
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void red_release_gpu(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier for a cooperative launch (all CTAs co-resident) on a
+// monotone arrival counter: barrier number n (0, 1, ...) completes when the
+// counter reaches (n + 1) * gridDim.x. Thread 0 arrives with a release
+// reduction and polls with acquire loads; the CTA barriers on either side
+// extend the ordering to the whole CTA. The wait is bounded (~2 s of
+// globaltimer): on expiry the CTA records CT_ERR_TIMEOUT in *status and
+// returns false; CTAs also leave once another CTA has recorded an error.
+// Callers must stop issuing work when this returns false.
+__device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int number, int32_t* status) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    volatile unsigned int* vgen = &bar->generation;
-    const unsigned int gen = *vgen;
-    __threadfence();
-    const unsigned int arrived = atomicAdd(&bar->count, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(&bar->count, 0u);
-      __threadfence();
-      atomicAdd(&bar->generation, 1u);
-    } else {
-      long long spins = 0;
-      while (*vgen == gen) {
+    const unsigned int target = (number + 1u) * gridDim.x;
+    red_release_gpu(&bar->count, 1u);
+    if (ld_acquire_gpu(&bar->count) < target) {
+      const unsigned long long t0 = global_ns();
+      while (ld_acquire_gpu(&bar->count) < target) {
         if (*(volatile int32_t*)status != 0) {
           ok = 0;
           break;
         }
-        if (++spins > kSpinLimit) {
+        if (global_ns() - t0 > 2000000000ull) {
           atomicCAS(status, 0, (int32_t)CT_ERR_TIMEOUT);
           ok = 0;
           break;
         }
-        __nanosleep(64);
       }
     }
-    __threadfence();
     s_ok = ok;
   }
   __syncthreads();

@@ -63,17 +63,27 @@ __global__ void roll_delays_kernel(float* __restrict__ coefs, int32_t* __restric
   delays[i] = d;
 }
 
+// dmin[0] = smallest, dmin[1] = largest delay of a connected (voxel, offset) pair
 __global__ void min_delay_kernel(const int32_t* __restrict__ nbr, const int32_t* __restrict__ delays, int64_t n,
                                  int32_t* __restrict__ dmin) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int32_t v = INT_MAX;
-  if (i < n && nbr[i] >= 0) v = delays[i];
+  int32_t lo = INT_MAX, hi = INT_MIN;
+  if (i < n && nbr[i] >= 0) lo = hi = delays[i];
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) v = min(v, __shfl_down_sync(0xffffffffu, v, off));
-  if ((threadIdx.x & 31) == 0 && v != INT_MAX) atomicMin(dmin, v);
+  for (int off = 16; off > 0; off >>= 1) {
+    lo = min(lo, __shfl_down_sync(0xffffffffu, lo, off));
+    hi = max(hi, __shfl_down_sync(0xffffffffu, hi, off));
+  }
+  if ((threadIdx.x & 31) == 0 && lo != INT_MAX) {
+    atomicMin(dmin, lo);
+    atomicMax(dmin + 1, hi);
+  }
 }
 
-__global__ void set_int_kernel(int32_t* p, int32_t v) { *p = v; }
+__global__ void set_min_max_kernel(int32_t* p) {
+  p[0] = INT_MAX;
+  p[1] = INT_MIN;
+}
 
 // ---- calculate_average_delays, derivation.rs:554-594
 __device__ __forceinline__ int offset_l1(int n) {
@@ -262,7 +272,7 @@ cudaError_t launch_update(DeviceScenario& d, const UpdateScalars& s, cudaStream_
 }
 
 cudaError_t launch_min_delay(DeviceScenario& d, cudaStream_t stream) {
-  set_int_kernel<<<1, 1, 0, stream>>>(d.dmin, INT_MAX);
+  set_min_max_kernel<<<1, 1, 0, stream>>>(d.dmin);
   const int64_t n = d.V * kOffsets;
   min_delay_kernel<<<blocks(n, 256), 256, 0, stream>>>(d.nbr, d.delays, n, d.dmin);
   return cudaGetLastError();
