@@ -171,14 +171,20 @@ class OracleEpoch:
                 setattr(s, name, int(val))
         return s
 
-    def run_epoch(self, algo: Algo, beat_order=None) -> None:
-        """One call of ``run_epoch`` (algorithm.rs:124-281)."""
+    def run_epoch(self, algo: Algo, beat_order=None, adjoint: bool = False) -> None:
+        """One call of ``run_epoch`` (algorithm.rs:124-281).
+
+        ``adjoint=True`` replaces the reference derivation by the exact
+        gradient of the stated loss (back-propagation through time); the
+        forward, metrics and update are unchanged.
+        """
         s = self._struct()
         order = None
         if beat_order is not None:
             order = np.ascontiguousarray(beat_order, dtype=np.int32)
         bi = ctypes.c_int64(self.batch_index)
-        fn = lib().oracle_run_epoch_f32 if self.dtype == np.float32 else lib().oracle_run_epoch_f64
+        kind = "adjoint_" if adjoint else ""
+        fn = getattr(lib(), f"oracle_run_epoch_{kind}{'f32' if self.dtype == np.float32 else 'f64'}")
         rc = fn(
             ctypes.byref(s),
             ctypes.byref(algo),
@@ -188,6 +194,21 @@ class OracleEpoch:
         if rc != 0:
             raise RuntimeError(f"oracle run_epoch failed with status {rc}")
         self.batch_index = bi.value
+
+    def stated_loss(self, algo: Algo, gradient: bool = False) -> float:
+        """Stated loss summed over beats, sum_t (mse/M)/2 |r|^2 + reg/2 sum_v relu(|x_v|_1 - thr)^2.
+
+        With ``gradient=True`` its exact gradient (plus the reference's
+        difference-regularisation term) is left in ``d_gains`` / ``d_coefs``.
+        f64 only.
+        """
+        if self.dtype != np.float64:
+            raise TypeError("stated_loss needs a float64 OracleEpoch")
+        s = self._struct()
+        fn = lib().oracle_adjoint_gradient_f64
+        fn.restype = ctypes.c_double
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        return float(fn(ctypes.addressof(s), ctypes.addressof(algo), int(gradient)))
 
     def simulate(self) -> np.ndarray:
         """Forward of every beat (simulation.rs:129-150); returns measurements [B,T,M]."""

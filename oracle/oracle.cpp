@@ -631,11 +631,172 @@ void simulate(Epoch<T>& e) {
   }
 }
 
+// ---------------------------------------------------------------- adjoint (no reference counterpart)
+//
+// Exact gradient of the stated loss of one beat,
+//   L_b = sum_t [ (mse/M) * 1/2 |r_t|^2 + reg * 1/2 * sum_v relu(|x_v|_1 - thr)^2 ],
+// by back-propagation through time over the forward recursion of
+// innovate_system_states (prediction.rs:40-86):
+//   ap[t] = c * (in_t - ap[t-1]) + in1_t,  in_t = x[t-d, j] (t >= d), in1_t = x[t-d-1, j] (t > d)
+//   x[t, i] = sum_k g[i,k] * ap[t] + u[t] * B[i].
+// Its instantaneous part at each step equals the reference's per-step factor
+// fma(mr, mse/M, mreg * reg) (derivation.rs:307-329); the 1/2 absorbs the 2
+// of the square. The difference-regularisation term is not a function of the
+// states: it is added as the reference's derivation adds it, once per (i, k)
+// pair per step it visits (textbook: all 9 pairs of (v, n), every step,
+// derivation.rs:484-497; simple: the 9 pairs of a connected (v, n) at steps
+// t >= d, derivation.rs:366-390), i.e. count * diff * delta^5.
+//
+// The all-pass outputs of (v, n, b) do not depend on the gain row's output
+// component a, so they are kept per voxel: aph[t][v][k], k = 3n + b.
+template <typename T>
+T adjoint_beat(Epoch<T>& e, const Algo& a, int64_t beat, bool want_grad) {
+  const int64_t S = e.num_states, V = e.num_voxels, M = e.num_sensors, Tn = e.num_steps;
+  const T mse_scaling = T(1) / static_cast<T>(M) * static_cast<T>(a.mse_strength);
+  const T reg = static_cast<T>(a.maximum_regularization_strength);
+  const T thr = static_cast<T>(a.maximum_regularization_threshold);
+  std::vector<T> aph((size_t)Tn * V * kGainCols);
+  estimations_reset(e);
+  T loss = 0;
+  for (int64_t t = 0; t < Tn; ++t) {
+    system_prediction(e, beat, t);
+    calculate_residuals(e, beat, t);
+    for (int64_t v = 0; v < V; ++v)
+      std::memcpy(&aph[((size_t)t * V + v) * kGainCols], e.ap_outputs_now + 3 * v * kGainCols, sizeof(T) * kGainCols);
+    T rr = 0;
+    for (int64_t m = 0; m < M; ++m) rr += e.residuals[m] * e.residuals[m];
+    T rg = 0;
+    const T* x = e.system_states + t * S;
+    for (int64_t v = 0; v < V; ++v) {
+      const T s = std::fabs(x[3 * v]) + std::fabs(x[3 * v + 1]) + std::fabs(x[3 * v + 2]);
+      if (s > thr) rg += (s - thr) * (s - thr);
+    }
+    loss += mse_scaling * T(0.5) * rr + reg * T(0.5) * rg;
+  }
+  if (!want_grad) return loss;
+
+  const T* H = e.measurement_matrix + beat * M * S;
+  std::vector<T> acc((size_t)Tn * S, T(0)), lam_x(S), lap((size_t)V * kGainCols, T(0)), r(M);
+  for (int64_t t = Tn - 1; t >= 0; --t) {
+    const T* x = e.system_states + t * S;
+    const T* y = e.measurements + (beat * Tn + t) * M;
+    const T* z = e.actual_measurements + (beat * Tn + t) * M;
+    for (int64_t m = 0; m < M; ++m) r[m] = y[m] - z[m];
+    for (int64_t v = 0; v < V; ++v) {
+      const T s = std::fabs(x[3 * v]) + std::fabs(x[3 * v + 1]) + std::fabs(x[3 * v + 2]);
+      const T f = s > thr ? s - thr : T(0);
+      for (int c = 0; c < 3; ++c) {
+        const int64_t i = 3 * v + c;
+        T mr = 0;
+        for (int64_t m = 0; m < M; ++m) mr += H[m * S + i] * r[m];
+        lam_x[i] = mse_scaling * mr + reg * f * signum(x[i]) + acc[(size_t)t * S + i];
+      }
+    }
+    for (int64_t v = 0; v < V; ++v) {
+      for (int n = 0; n < kOffsets; ++n) {
+        const int32_t out0 = e.output_state_indices[(3 * v) * kGainCols + 3 * n];
+        if (out0 < 0) continue;
+        const int64_t ci = v * kOffsets + n;
+        const T c = e.coefs[ci];
+        const int64_t d = e.delays[ci];
+        for (int b = 0; b < 3; ++b) {
+          const int k = 3 * n + b;
+          const int64_t j = out0 + b;  // state index 3 * neighbour + b
+          T G = 0;
+          for (int c3 = 0; c3 < 3; ++c3) G += e.gains[(3 * v + c3) * kGainCols + k] * lam_x[3 * v + c3];
+          const T lnew = G - c * lap[v * kGainCols + k];
+          const T ap_t = aph[((size_t)t * V + v) * kGainCols + k];
+          const T ap_prev = t > 0 ? aph[((size_t)(t - 1) * V + v) * kGainCols + k] : T(0);
+          const T in = (d <= t) ? e.system_states[(t - d) * S + j] : T(0);
+          if (!a.freeze_gains)
+            for (int c3 = 0; c3 < 3; ++c3) e.d_gains[(3 * v + c3) * kGainCols + k] += lam_x[3 * v + c3] * ap_t;
+          if (!a.freeze_delays) e.d_coefs[ci] += lnew * (in - ap_prev);
+          if (t - d >= 0) acc[(size_t)(t - d) * S + j] += c * lnew;
+          if (t - d - 1 >= 0) acc[(size_t)(t - d - 1) * S + j] += lnew;
+          lap[v * kGainCols + k] = lnew;
+        }
+      }
+    }
+  }
+  if (!a.freeze_delays) {
+    const T diff = static_cast<T>(a.difference_regularization_strength);
+    for (int64_t v = 0; v < V; ++v)
+      for (int n = 0; n < kOffsets; ++n) {
+        const int64_t ci = v * kOffsets + n;
+        int64_t count = 9 * Tn;
+        if (a.ap_derivative == 0) {
+          const bool connected = e.output_state_indices[(3 * v) * kGainCols + 3 * n] >= 0;
+          count = connected ? 9 * std::max<int64_t>(0, Tn - e.delays[ci]) : 0;
+        }
+        e.d_coefs[ci] += static_cast<T>(count) * (diff * delay_delta(e, ci));
+      }
+  }
+  return loss;
+}
+
+// run_epoch (algorithm.rs:124-281) with the derivation replaced by the
+// adjoint: the forward, residuals, maximum-regularisation sum and metrics of
+// every step are the reference's; gradients come from adjoint_beat.
+template <typename T>
+int run_epoch_adjoint(Epoch<T>& e, const Algo& a, const int32_t* beat_order, int64_t* batch_index) {
+  derivatives_reset(e);
+  const T reg = static_cast<T>(a.maximum_regularization_strength);
+  int64_t batch = 0;
+  const bool batched = a.batch_size != 0;
+  for (int64_t bi = 0; bi < e.num_beats; ++bi) {
+    const int64_t beat = beat_order ? beat_order[bi] : bi;
+    if (beat < 0 || beat >= e.num_beats) return -2;
+    adjoint_beat(e, a, beat, true);
+    // metrics of the beat's forward (system_states of this beat are in place)
+    for (int64_t step = 0; step < e.num_steps; ++step) {
+      predict_measurements(e, beat, step);
+      calculate_residuals(e, beat, step);
+      calculate_mapped_residuals(e, beat, step);
+      calculate_maximum_regularization(e, step, static_cast<T>(a.maximum_regularization_threshold));
+      metrics_step(e, reg, step);
+    }
+    if (batched) {
+      batch += 1;
+      if (batch == a.batch_size) {
+        int rc = batch_end(e, a, batch, batch_index);
+        if (rc) return rc;
+        derivatives_reset(e);
+        batch = 0;
+      }
+    }
+  }
+  if (batched) {
+    if (batch > 0) return batch_end(e, a, batch, batch_index);
+    return 0;
+  }
+  return batch_end(e, a, e.num_beats, batch_index);
+}
+
+// Stated loss summed over beats and its gradient (accumulated into d_gains /
+// d_coefs after a reset); no update.
+template <typename T>
+T adjoint_gradient(Epoch<T>& e, const Algo& a, bool want_grad) {
+  if (want_grad) derivatives_reset(e);
+  T loss = 0;
+  for (int64_t beat = 0; beat < e.num_beats; ++beat) loss += adjoint_beat(e, a, beat, want_grad);
+  return loss;
+}
+
 }  // namespace
 
 extern "C" {
 
 int oracle_abi_version() { return 1; }
+
+int oracle_run_epoch_adjoint_f64(Epoch<double>* e, const Algo* a, const int32_t* beat_order, int64_t* batch_index) {
+  return run_epoch_adjoint(*e, *a, beat_order, batch_index);
+}
+int oracle_run_epoch_adjoint_f32(Epoch<float>* e, const Algo* a, const int32_t* beat_order, int64_t* batch_index) {
+  return run_epoch_adjoint(*e, *a, beat_order, batch_index);
+}
+double oracle_adjoint_gradient_f64(Epoch<double>* e, const Algo* a, int want_grad) {
+  return adjoint_gradient(*e, *a, want_grad != 0);
+}
 
 int oracle_run_epoch_f32(Epoch<float>* e, const Algo* a, const int32_t* beat_order, int64_t* batch_index) {
   return run_epoch(*e, *a, beat_order, batch_index);
