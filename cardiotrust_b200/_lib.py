@@ -74,6 +74,7 @@ EXPORTED = [
     "ct_scenario_destroy",
     "ct_scenario_dims",
     "ct_run_epoch",
+    "ct_run_epoch_plain",
     "ct_simulate",
     "ct_set_algorithm",
     "ct_set_freeze",
@@ -157,6 +158,7 @@ def load(path: pathlib.Path = LIB_PATH) -> ctypes.CDLL:
     lib.ct_scenario_destroy.argtypes = [vp]
     lib.ct_scenario_dims.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int64)] * 4
     lib.ct_run_epoch.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), _ip, ctypes.c_int, ctypes.c_int]
+    lib.ct_run_epoch_plain.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), _ip]
     lib.ct_simulate.argtypes = [vp, _fp, _fp]
     lib.ct_set_algorithm.argtypes = [vp, ctypes.POINTER(CtAlgorithm)]
     lib.ct_set_freeze.argtypes = [vp, ctypes.c_int, ctypes.c_int]

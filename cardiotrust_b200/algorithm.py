@@ -38,7 +38,8 @@ class APDerivative(enum.IntEnum):
 
 
 class GradMode(enum.IntEnum):
-    Reference = 0
+    Reference = 0  # the reference's per-step derivation (derivation.rs:173-229)
+    Adjoint = 1  # exact gradient of the stated loss, back-propagation through time with checkpoints
 
 
 class Precision(enum.IntEnum):
@@ -199,6 +200,16 @@ class EpochEngine:
         order = None if beat_order is None else _i32(beat_order)
         check(lib().ct_run_epoch(self._h, ctypes.byref(bi), None if order is None else iptr(order), int(grad_mode),
                                  int(precision)))
+        if sync:
+            self.sync()
+        return bi.value
+
+    def run_epoch_plain(self, batch_index: int = 0, beat_order=None, sync: bool = True) -> int:
+        """The plain GPU form of :meth:`run_epoch` (reference gradients, FP32): one kernel launch per
+        phase per step, one scenario at a time - the baseline the persistent form is measured against."""
+        bi = ctypes.c_int64(int(batch_index))
+        order = None if beat_order is None else _i32(beat_order)
+        check(lib().ct_run_epoch_plain(self._h, ctypes.byref(bi), None if order is None else iptr(order)))
         if sync:
             self.sync()
         return bi.value

@@ -47,6 +47,11 @@ struct ct_scn {
   uint64_t rng = 0x9e3779b97f4a7c15ull;
   std::vector<void*> allocations;
   std::vector<int32_t> nbr_host;  // neighbour table in reference order, for validating delay writes
+  std::vector<int32_t> nbr_dev;   // neighbour table in device order (adjoint reverse table)
+  // Upper bound of the largest delay of a connected pair: exact after creation and delay writes,
+  // +1 per update that rolls delays (roll_delays moves a delay by at most one). Sizes the
+  // adjoint ring without reading the device.
+  int64_t dmax_bound = 1;
   // Device voxel order: device voxel u holds reference voxel perm[u]; inv is the inverse.
   std::vector<int32_t> perm, inv;
   // launch accounting and optional per-phase CUDA-event timing
@@ -152,12 +157,81 @@ void seeded_shuffle(ct_scn* s, std::vector<int32_t>& order) {
   }
 }
 
-int run_beat(ct_scn* s, int64_t beat, int precision) {
+int64_t max_connected_delay(const std::vector<int32_t>& nbr, const int32_t* delays) {
+  int64_t m = 1;
+  for (size_t i = 0; i < nbr.size(); ++i)
+    if (nbr[i] >= 0 && delays[i] > m) m = delays[i];
+  return m;
+}
+
+void release(ct_scn* s, void* p) {
+  if (!p) return;
+  cudaFree(p);
+  s->allocations.erase(std::remove(s->allocations.begin(), s->allocations.end(), p), s->allocations.end());
+}
+
+// Adjoint-mode buffers, allocated on first use; the ring grows with the delay bound.
+int prepare_adjoint(ct_scn* s) {
+  DeviceScenario& d = s->d;
+  cudaStream_t st = s->ctx->stream;
+  const int64_t V = d.V, plane = d.V * kGainCols;
+  if (!d.rev) {
+    std::vector<int32_t> rev((size_t)(V * kOffsets), -1);
+    for (int64_t v = 0; v < V; ++v)
+      for (int n = 0; n < kOffsets; ++n) {
+        const int32_t j = s->nbr_dev[(size_t)(v * kOffsets + n)];
+        if (j < 0) continue;
+        int32_t& slot = rev[(size_t)j * kOffsets + n];
+        if (slot >= 0)
+          return fail(CT_ERR_NOT_SUPPORTED,
+                      "adjoint mode: two voxels reach the same neighbour along one offset (not a lattice)");
+        slot = (int32_t)v;
+      }
+    const int64_t nseg = (d.T + ct::kCkptSteps - 1) / ct::kCkptSteps;
+    const int64_t seg_steps = std::min<int64_t>(d.T, ct::kCkptSteps);
+    int rc = alloc(s, &d.rev, V * kOffsets);
+    if (!rc) rc = alloc(s, &d.ckpt, nseg * plane);
+    if (!rc) rc = alloc(s, &d.seg_ap, seg_steps * plane);
+    if (!rc) rc = alloc(s, &d.seg_q, seg_steps * plane);
+    if (!rc) rc = alloc(s, &d.dCk, plane);
+    if (rc) {
+      for (void* p : {(void*)d.rev, (void*)d.ckpt, (void*)d.seg_ap, (void*)d.seg_q, (void*)d.dCk}) release(s, p);
+      d.rev = nullptr;
+      d.ckpt = d.seg_ap = d.seg_q = d.dCk = nullptr;
+      return rc;
+    }
+    CT_CUDA(cudaMemcpyAsync(d.rev, rev.data(), sizeof(int32_t) * rev.size(), cudaMemcpyHostToDevice, st),
+            "upload reverse table");
+    CT_CUDA(cudaMemsetAsync(d.ckpt, 0, sizeof(float) * nseg * plane, st), "memset");
+    CT_CUDA(cudaMemsetAsync(d.dCk, 0, sizeof(float) * plane, st), "memset");
+    CT_CUDA(cudaStreamSynchronize(st), "adjoint set-up");
+    d.adj_grid = (int)std::min<int64_t>((V + ct::kFwdTileVoxels - 1) / ct::kFwdTileVoxels,
+                                        ct::adjoint_capacity(s->ctx->device));
+  }
+  int need = 1;
+  while (need < s->dmax_bound + ct::kMaxStepBlock + 2) need <<= 1;
+  if (!d.lam || d.adj_ring < need) {
+    CT_CUDA(cudaStreamSynchronize(st), "adjoint ring");
+    release(s, d.lam);
+    d.lam = nullptr;
+    d.adj_ring = 0;
+    int rc = alloc(s, &d.lam, (int64_t)need * plane);
+    if (rc) return rc;
+    d.adj_ring = need;
+  }
+  return CT_OK;
+}
+
+int run_beat(ct_scn* s, int64_t beat, int precision, int grad_mode) {
   DeviceScenario& d = s->d;
   const ct_algorithm& a = s->algo;
   cudaStream_t st = s->ctx->stream;
+  const bool adjoint = grad_mode == CT_GRAD_ADJOINT;
   CT_CUDA(run_phase(s, CT_PHASE_FORWARD, 1,
-                    [&] { return ct::launch_forward(d, a.maximum_regularization_threshold, st); }),
+                    [&] {
+                      return ct::launch_forward(d, a.maximum_regularization_threshold, adjoint ? d.ckpt : nullptr,
+                                                st);
+                    }),
           "forward kernel");
   if (precision == CT_PREC_FP32) {
     CT_CUDA(run_phase(s, CT_PHASE_MEASURE, 3, [&] { return ct::launch_measure(d, beat, true, st); }),
@@ -172,7 +246,17 @@ int run_beat(ct_scn* s, int64_t beat, int precision) {
                       [&] { return ct::launch_map_residuals_umma(d, beat, precision, st); }),
             "tensor-core mapped-residual kernel");
   }
-  if (!a.freeze_gains || !a.freeze_delays) {
+  if (adjoint && (!a.freeze_gains || !a.freeze_delays)) {
+    ct::AdjointScalars as;
+    as.mse_scaling = 1.0f / (float)d.M * a.mse_strength;
+    as.reg_scaling = a.maximum_regularization_strength;
+    as.threshold = a.maximum_regularization_threshold;
+    as.diffreg = a.difference_regularization_strength;
+    as.freeze_gains = a.freeze_gains;
+    as.freeze_delays = a.freeze_delays;
+    as.ap_derivative = a.ap_derivative;
+    CT_CUDA(run_phase(s, CT_PHASE_DERIVE, 1, [&] { return ct::launch_adjoint(d, as, st); }), "adjoint kernel");
+  } else if (!a.freeze_gains || !a.freeze_delays) {
     ct::DeriveScalars ds;
     ds.mse_scaling = 1.0f / (float)d.M * a.mse_strength;
     ds.reg_scaling = a.maximum_regularization_strength;
@@ -235,6 +319,7 @@ int batch_end(ct_scn* s, int64_t n_beats, int64_t* batch_index) {
   return ct::launch_batch_metrics(d, *batch_index, st);
   });
   if (err != cudaSuccess) return cuda_fail(err, "update kernels");
+  if (!a.freeze_delays) s->dmax_bound = std::min<int64_t>(s->dmax_bound + 1, 1000);
   s->adam_step += 1;
   *batch_index += 1;
   return CT_OK;
@@ -605,6 +690,7 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   s->ctx = ctx;
   s->algo = *algo;
   s->nbr_host = nbr;
+  s->dmax_bound = max_connected_delay(nbr, desc->delays);
   brick_layout(nbr, S / 3, s->perm, s->inv);
   DeviceScenario& d = s->d;
   d.S = S;
@@ -711,6 +797,7 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
       const int32_t w = nbr[(size_t)s->perm[(size_t)u] * kOffsets + n];
       h_nbr[(size_t)(u * kOffsets + n)] = w < 0 ? -1 : s->inv[(size_t)w];
     }
+  s->nbr_dev = h_nbr;
   r = r ? r : upload(s, d.gains, h_gains.data(), sizeof(float) * S * kGainCols);
   r = r ? r : upload(s, d.nbr, h_nbr.data(), sizeof(int32_t) * V * kOffsets);
   r = r ? r : upload(s, d.coefs, h_coefs.data(), sizeof(float) * V * kOffsets);
@@ -801,9 +888,33 @@ int ct_scenario_dims(ct_scn* scn, int64_t* S, int64_t* M, int64_t* T, int64_t* B
   return CT_OK;
 }
 
-int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, int grad_mode, int precision) {
+static int run_beat_plain(ct_scn* s, int64_t beat) {
+  DeviceScenario& d = s->d;
+  const ct_algorithm& a = s->algo;
+  if (!d.plain_mreg) {
+    int rc = alloc(s, &d.plain_mreg, d.S);
+    if (!rc) rc = alloc(s, &d.plain_part, (d.V + 255) / 256);
+    if (rc) return rc;
+  }
+  ct::PlainScalars ps;
+  ps.mse_scaling = 1.0f / (float)d.M * a.mse_strength;
+  ps.reg_scaling = a.maximum_regularization_strength;
+  ps.threshold = a.maximum_regularization_threshold;
+  ps.diffreg = a.difference_regularization_strength;
+  ps.freeze_gains = a.freeze_gains;
+  ps.freeze_delays = a.freeze_delays;
+  ps.ap_derivative = a.ap_derivative;
+  CT_CUDA(run_phase(s, CT_PHASE_FORWARD, (int)(d.T * ct::plain_step_launches(ps)),
+                    [&] { return ct::launch_plain_beat(d, beat, ps, s->ctx->stream); }),
+          "plain-form kernels");
+  return CT_OK;
+}
+
+static int run_epoch_impl(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, int grad_mode,
+                          int precision, bool plain) {
   if (!scn || !batch_index) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
-  if (grad_mode != CT_GRAD_REFERENCE) return fail(CT_ERR_NOT_SUPPORTED, "gradient mode %d", grad_mode);
+  if (grad_mode != CT_GRAD_REFERENCE && grad_mode != CT_GRAD_ADJOINT)
+    return fail(CT_ERR_NOT_SUPPORTED, "gradient mode %d", grad_mode);
   if (precision != CT_PREC_FP32 && precision != CT_PREC_TF32X3 && precision != CT_PREC_TF32)
     return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
   if (precision != CT_PREC_FP32 && !scn->d.umma)
@@ -824,10 +935,14 @@ int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, i
   }
   int rc = derivatives_reset(scn);
   if (rc) return rc;
+  if (grad_mode == CT_GRAD_ADJOINT && (!a.freeze_gains || !a.freeze_delays)) {
+    rc = prepare_adjoint(scn);
+    if (rc) return rc;
+  }
   int64_t batch = 0;
   const bool batched = a.batch_size != 0;
   for (int32_t beat : order) {
-    rc = run_beat(scn, beat, precision);
+    rc = plain ? run_beat_plain(scn, beat) : run_beat(scn, beat, precision, grad_mode);
     if (rc) return rc;
     if (batched) {
       batch += 1;
@@ -844,6 +959,14 @@ int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, i
   return batch_end(scn, d.B, batch_index);
 }
 
+int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, int grad_mode, int precision) {
+  return run_epoch_impl(scn, batch_index, beat_order, grad_mode, precision, false);
+}
+
+int ct_run_epoch_plain(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order) {
+  return run_epoch_impl(scn, batch_index, beat_order, CT_GRAD_REFERENCE, CT_PREC_FP32, true);
+}
+
 int ct_simulate(ct_scn* scn, float* measurements_out, float* states_out) {
   if (!scn || !measurements_out) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
   CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
@@ -851,7 +974,7 @@ int ct_simulate(ct_scn* scn, float* measurements_out, float* states_out) {
   cudaStream_t st = scn->ctx->stream;
   for (int64_t beat = 0; beat < d.B; ++beat) {
     CT_CUDA(run_phase(scn, CT_PHASE_FORWARD, 1,
-                      [&] { return ct::launch_forward(d, scn->algo.maximum_regularization_threshold, st); }),
+                      [&] { return ct::launch_forward(d, scn->algo.maximum_regularization_threshold, nullptr, st); }),
             "forward kernel");
     CT_CUDA(run_phase(scn, CT_PHASE_MEASURE, 2, [&] { return ct::launch_measure(d, beat, false, st); }),
             "measurement kernel");
@@ -960,6 +1083,7 @@ int ct_write_field(ct_scn* scn, int field, const void* src, size_t nbytes) {
         if (nbr[i] >= 0 && del[i] < 1)
           return fail(CT_ERR_INVALID_ARGUMENT, "delay %zu of a connected pair is %d; delays must be >= 1", i, del[i]);
       dst = d.delays;
+      scn->dmax_bound = max_connected_delay(nbr, del);
       break;
     }
     case CT_FIELD_MEASUREMENTS_ACTUAL: dst = d.meas; break;

@@ -13,6 +13,7 @@ constexpr int kGainCols = 78;  // 26 offsets x 3 neighbour components
 constexpr int kMaxStepBlock = 8;  // steps advanced between grid barriers in the forward kernel
 constexpr int kFwdTileVoxels = 32;  // voxels per forward tile (consecutive in device order)
 constexpr int kFwdHaloMax = 160;    // largest neighbourhood of a tile the resident forward form stages
+constexpr int kCkptSteps = 256;     // adjoint mode: all-pass state checkpoint interval (power of two)
 
 // Device-side grid barrier state: a monotone arrival counter, zeroed before each launch.
 struct GridBarrier {
@@ -70,6 +71,18 @@ struct DeviceScenario {
   int32_t* halo;         // [tiles, kFwdHaloMax] device voxels of each tile's neighbourhood
   int16_t* hslot;        // [tiles, 26 * kFwdTileVoxels] halo slot of each item's neighbour, -1 if absent
   int32_t* nhalo;        // [tiles]
+  // adjoint mode (ct_adjoint.cu), allocated on first use
+  int32_t* rev;          // [V,26] voxel whose offset n points at this voxel, -1 if none
+  float* ckpt;           // [ceil(T/kCkptSteps), V, 78] all-pass state before step s * kCkptSteps
+  float* seg_ap;         // [kCkptSteps, V, 78] recomputed all-pass outputs of one segment
+  float* seg_q;          // [kCkptSteps, V, 78] in_t - ap[t-1] of one segment
+  float* lam;            // [adj_ring, V, 78] adjoint all-pass values of recent steps
+  float* dCk;            // [V,78] per-column coefficient-gradient partials
+  int adj_ring;          // ring slots (power of two)
+  int adj_grid;          // CTAs of the adjoint kernel
+  // plain form (ct_plain.cu), allocated on first use
+  float* plain_mreg;     // [S] maximum regularisation of the current step
+  float* plain_part;     // [ceil(V / 256)] per-block sums of the step's regularisation terms
   int32_t* status;       // [1] device-side error code (0 = ok)
   GridBarrier* barrier;  // [1]
 };
@@ -79,8 +92,9 @@ int report_error(int status, const char* message);
 
 // ---- launchers (all enqueue on `stream`, return cudaError_t of the launch)
 
-// Forward propagation of one beat: X[t,:] for t in [0,T).
-cudaError_t launch_forward(DeviceScenario& d, float threshold, cudaStream_t stream);
+// Forward propagation of one beat: X[t,:] for t in [0,T). With ckpt non-null the all-pass
+// state before every step s * kCkptSteps (s >= 1) is stored in ckpt[s].
+cudaError_t launch_forward(DeviceScenario& d, float threshold, float* ckpt, cudaStream_t stream);
 // CTAs of the streaming form, and how many CTAs of the resident form fit on the device.
 int forward_grid_size(int64_t V, int device);
 int forward_ring_capacity(int device);
@@ -107,6 +121,23 @@ struct DeriveScalars {
 };
 // Per-(voxel, offset) sweep over the steps of one beat: dG, dC, fir, iir.
 cudaError_t launch_derive(DeviceScenario& d, const DeriveScalars& s, cudaStream_t stream);
+
+struct AdjointScalars {
+  float mse_scaling, reg_scaling, threshold, diffreg;
+  int freeze_gains, freeze_delays, ap_derivative;
+};
+// Back-propagation through time of one beat (needs X, MR and the forward's checkpoints): dG, dC.
+cudaError_t launch_adjoint(DeviceScenario& d, const AdjointScalars& s, cudaStream_t stream);
+// How many CTAs of the adjoint kernel fit on the device at once.
+int adjoint_capacity(int device);
+
+struct PlainScalars {
+  float mse_scaling, reg_scaling, threshold, diffreg;
+  int freeze_gains, freeze_delays, ap_derivative;
+};
+// Plain form of one beat (prediction, reference derivation and step metrics), launched per step.
+cudaError_t launch_plain_beat(DeviceScenario& d, int64_t beat, const PlainScalars& s, cudaStream_t stream);
+int plain_step_launches(const PlainScalars& s);
 
 // Step metrics of one beat: loss_mr[t] (running), loss[t]; advances mreg_sum.
 cudaError_t launch_step_metrics(DeviceScenario& d, float reg_strength, cudaStream_t stream);

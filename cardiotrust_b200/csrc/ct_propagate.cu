@@ -66,6 +66,7 @@ struct FwdArgs {
   float* ap;
   float* ap_last;
   float* stepsum_part;
+  float* ckpt;  // adjoint checkpoints [ceil(T / kCkptSteps), V, 78] or null
   const int32_t* dmin;
   float threshold;
   int32_t* status;
@@ -175,6 +176,8 @@ __device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int 
             a = fmaf(c, h[i][s + 1][b] - a, h[i][s][b]);
             out0[s * (kTileVoxels * kGainCols) + b] = a;
             if (tr0 + s == p.T - 2) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = a;
+            if (p.ckpt && ((tr0 + s + 1) & (kCkptSteps - 1)) == 0 && tr0 + s + 1 < p.T)
+              p.ckpt[((size_t)((tr0 + s + 1) / kCkptSteps) * p.V + v0 + vl) * kGainCols + 3 * n + b] = a;
           }
         }
         st[b] = a;
@@ -472,6 +475,8 @@ __global__ void __launch_bounds__(kThreads, 1) forward_ring_kernel(FwdArgs p, Ri
                   a = fmaf(cc[i], h[s2 + 1][b] - a, h[s2][b]);
                   out0[s2 * (kTileVoxels * kGainCols) + b] = a;
                   if (tr0 + s2 == T - 2) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = a;
+                  if (p.ckpt && ((tr0 + s2 + 1) & (kCkptSteps - 1)) == 0 && tr0 + s2 + 1 < T)
+                    p.ckpt[((size_t)((tr0 + s2 + 1) / kCkptSteps) * p.V + v0 + vl) * kGainCols + 3 * n + b] = a;
                 }
               }
               st[i][b] = a;
@@ -577,7 +582,7 @@ int forward_ring_capacity(int device) {
   return sms * per_sm;
 }
 
-cudaError_t launch_forward(DeviceScenario& d, float threshold, cudaStream_t stream) {
+cudaError_t launch_forward(DeviceScenario& d, float threshold, float* ckpt, cudaStream_t stream) {
   FwdArgs a;
   a.V = (int)d.V;
   a.S = (int)d.S;
@@ -592,6 +597,7 @@ cudaError_t launch_forward(DeviceScenario& d, float threshold, cudaStream_t stre
   a.ap = d.ap;
   a.ap_last = d.ap_last;
   a.stepsum_part = d.stepsum_part;
+  a.ckpt = ckpt;
   a.dmin = d.dmin;
   a.threshold = threshold;
   a.status = d.status;

@@ -52,7 +52,12 @@ enum ct_optimizer { CT_OPT_SGD = 0, CT_OPT_ADAM = 1 };
 enum ct_ap_derivative { CT_AP_SIMPLE = 0, CT_AP_TEXTBOOK = 1 };
 /* Gradient definition used by ct_run_epoch. */
 enum ct_grad_mode {
-  CT_GRAD_REFERENCE = 0 /* the reference's per-step derivation, derivation.rs:173-229 */
+  CT_GRAD_REFERENCE = 0, /* the reference's per-step derivation, derivation.rs:173-229 */
+  /* Exact gradient of the stated loss sum_t (mse/M)/2 |r_t|^2 + reg/2 sum_v relu(|x_v|_1 - thr)^2
+   * by back-propagation through time (no counterpart in the reference), plus the reference's
+   * difference-regularisation term. All-pass state is checkpointed every 256 steps and the
+   * segments in between are recomputed. Forward, metrics and update are those of mode 0. */
+  CT_GRAD_ADJOINT = 1
 };
 /* Arithmetic of the two measurement products (H x and H^T r). */
 enum ct_precision {
@@ -154,8 +159,19 @@ int ct_scenario_dims(ct_scn* scn, int64_t* S, int64_t* M, int64_t* T, int64_t* B
 /* One estimation epoch, enqueued on the context stream (asynchronous).
  * beat_order: B beat indices, or NULL for the library's seeded shuffle.
  * batch_index: in/out batch-wise metric cursor (algorithm.rs:126).
+ * grad_mode: ct_grad_mode. CT_GRAD_ADJOINT allocates its checkpoint and segment buffers on
+ * first use (about (T/256 + 256 * 2 + ring) x V x 78 floats) and needs every voxel pair to be
+ * connected along at most one offset (true of the reference's lattice).
  * Device-side failures are reported by ct_sync. */
 int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, int grad_mode, int precision);
+
+/* The plain GPU form of ct_run_epoch (CT_GRAD_REFERENCE, FP32 products): every phase of every
+ * step is its own kernel launch with one thread per output, one scenario at a time - the
+ * straightforward port of the reference's OpenCL epoch (src/core/algorithm/gpu/epoch.rs:96-117,
+ * prediction/derivation/metrics kernels per step). Kept as the baseline the persistent and
+ * batched forms are measured against. Same arguments, results (within tolerance) and error
+ * behaviour as ct_run_epoch. */
+int ct_run_epoch_plain(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order);
 
 /* Forward of every beat with the current parameters (no noise); writes the predicted
  * measurements [B,T,M] and, if non-NULL, the states [T,S] of the last beat. Synchronous. */
