@@ -323,71 +323,93 @@ def _delay_samples(types, numbers, positions, velocity, sample_rate) -> np.ndarr
 def _connect_voxels(types, numbers, positions, velocity, current_factor_in_pathology):
     """Activation-front search of connect_voxels / try_to_connect (allpass.rs:295-494).
 
+    The reference visits activation times in increasing order; at each time
+    ``current`` it takes a snapshot of the activated voxels whose time is
+    relative_eq to ``current`` and lets each of them, in C order, activate
+    its not yet activated neighbours (first come, first served). Here the
+    activated-but-unvisited voxels sit in a heap keyed by time, so each
+    snapshot is popped instead of found by a scan of the whole grid; a
+    voxel activated while a snapshot is processed waits for a later one, as
+    in the reference. Distances, directions and gains depend only on the
+    position difference of the pair and the output voxel's direction, and
+    are cached on those keys.
+
     Returns (gains [S,78], activation_time_ms [nx,ny,nz]).
     """
+    import heapq
+
     nx, ny, nz = types.shape
     S = int((numbers >= 0).sum()) * 3
     gains = np.zeros((S, 78), dtype=np.float32)
     act = np.full(types.shape, np.nan, dtype=np.float32)
     dirs = np.zeros(types.shape + (3,), dtype=np.float32)
-    current = np.float32(0.0)
-    sa = np.argwhere(types == VT_SINOATRIAL)
-    for idx in sa:
-        act[tuple(idx)] = current
-        dirs[tuple(idx)] = np.array([1.0, 0.0, 0.0], dtype=np.float32)
     patho_zero = abs(current_factor_in_pathology) <= F32_EPS or abs(current_factor_in_pathology) == 0.0
-    connected_something = True
-    while connected_something:
-        valid = ~np.isnan(act)
-        if not np.any(act[valid] > current):
-            connected_something = False
-        cand = np.argwhere(valid & _relative_eq(np.nan_to_num(act, nan=np.inf), current))
-        for out_idx in cand:  # argwhere is C-order, as indexed_iter
-            xo, yo, zo = (int(c) for c in out_idx)
+    types_l = types.tolist()
+    numbers_l = numbers.tolist()
+    heap = []  # (time, C-order index) of activated voxels not visited yet
+    for idx in np.argwhere(types == VT_SINOATRIAL):
+        act[tuple(idx)] = np.float32(0.0)
+        dirs[tuple(idx)] = np.array([1.0, 0.0, 0.0], dtype=np.float32)
+        heapq.heappush(heap, (0.0, int(np.ravel_multi_index(tuple(idx), types.shape))))
+    pair_cache = {}
+    gain_cache = {}
+    offsets = [(ox, oy, oz) for ox in (-1, 0, 1) for oy in (-1, 0, 1) for oz in (-1, 0, 1) if (ox, oy, oz) != (0, 0, 0)]
+    col = {(ox, oy, oz): offset_to_gain_index(ox, oy, oz, 0) for (ox, oy, oz) in offsets}
+    f_in = np.float32(current_factor_in_pathology)
+    f_out = np.float32(np.float32(1.0) / np.float32(current_factor_in_pathology)) if not patho_zero else None
+    while heap:
+        current = np.float32(heap[0][0])
+        tol = max(float(F32_EPS), abs(float(current)) * float(F32_EPS))
+        snap = []
+        while heap and (heap[0][0] - float(current)) <= tol:
+            snap.append(heapq.heappop(heap)[1])
+        snap.sort()  # C order, as indexed_iter
+        for flat in snap:
+            xo, yo, zo = np.unravel_index(flat, types.shape)
+            xo, yo, zo = int(xo), int(yo), int(zo)
             t_out = act[xo, yo, zo]
-            type_out = int(types[xo, yo, zo])
-            for ox in (-1, 0, 1):
-                for oy in (-1, 0, 1):
-                    for oz in (-1, 0, 1):
-                        if ox == 0 and oy == 0 and oz == 0:
-                            continue
-                        xi, yi, zi = xo - ox, yo - oy, zo - oz
-                        if not (0 <= xi < nx and 0 <= yi < ny and 0 <= zi < nz):
-                            continue
-                        type_in = int(types[xi, yi, zi])
-                        if type_in not in _CONNECTABLE:
-                            continue
-                        if not np.isnan(act[xi, yi, zi]):
-                            continue
-                        if type_in not in _ALLOWED_INPUTS.get(type_out, set()) and type_out != VT_PATHOLOGICAL:
-                            continue
-                        if type_out not in _CONNECTABLE or type_out in (VT_NONE,):
-                            continue
-                        if type_in == VT_PATHOLOGICAL and patho_zero:
-                            continue
-                        p_in = positions[xi, yi, zi]
-                        p_out = positions[xo, yo, zo]
-                        ds = _delay_s(p_in, p_out, velocity)
-                        act[xi, yi, zi] = np.float32(t_out + ds)
-                        direction = _direction(p_in, p_out)
-                        dirs[xi, yi, zi] = direction
-                        g = _gain(direction, dirs[xo, yo, zo])
-                        if type_in == VT_PATHOLOGICAL and type_out != VT_PATHOLOGICAL:
-                            g = (g * np.float32(current_factor_in_pathology)).astype(np.float32)
-                        if type_out == VT_PATHOLOGICAL and type_in != VT_PATHOLOGICAL:
-                            g = (g * np.float32(np.float32(1.0) / np.float32(current_factor_in_pathology))).astype(
-                                np.float32
-                            )
-                        base = int(numbers[xi, yi, zi])
-                        for i in range(3):
-                            for o in range(3):
-                                gains[base + i, offset_to_gain_index(ox, oy, oz, o)] = g[i, o]
-                        connected_something = True
-        later = act[~np.isnan(act)]
-        later = later[later > current]
-        if later.size == 0:
-            break
-        current = np.float32(later.min())
+            type_out = types_l[xo][yo][zo]
+            if type_out not in _CONNECTABLE:
+                continue
+            dir_out = dirs[xo, yo, zo]
+            dir_key = dir_out.tobytes()
+            for ox, oy, oz in offsets:
+                xi, yi, zi = xo - ox, yo - oy, zo - oz
+                if not (0 <= xi < nx and 0 <= yi < ny and 0 <= zi < nz):
+                    continue
+                type_in = types_l[xi][yi][zi]
+                if type_in not in _CONNECTABLE:
+                    continue
+                if not np.isnan(act[xi, yi, zi]):
+                    continue
+                if type_in not in _ALLOWED_INPUTS.get(type_out, set()) and type_out != VT_PATHOLOGICAL:
+                    continue
+                if type_in == VT_PATHOLOGICAL and patho_zero:
+                    continue
+                p_in = positions[xi, yi, zi]
+                p_out = positions[xo, yo, zo]
+                dkey = (p_in - p_out).tobytes()
+                pr = pair_cache.get(dkey)
+                if pr is None:
+                    pr = (_delay_s(p_in, p_out, velocity), _direction(p_in, p_out))
+                    pair_cache[dkey] = pr
+                ds, direction = pr
+                t_in = np.float32(t_out + ds)
+                act[xi, yi, zi] = t_in
+                dirs[xi, yi, zi] = direction
+                gkey = (dkey, dir_key)
+                g = gain_cache.get(gkey)
+                if g is None:
+                    g = _gain(direction, dir_out)
+                    gain_cache[gkey] = g
+                if type_in == VT_PATHOLOGICAL and type_out != VT_PATHOLOGICAL:
+                    g = (g * f_in).astype(np.float32)
+                if type_out == VT_PATHOLOGICAL and type_in != VT_PATHOLOGICAL:
+                    g = (g * f_out).astype(np.float32)
+                base = numbers_l[xi][yi][zi]
+                c0 = col[(ox, oy, oz)]
+                gains[base:base + 3, c0:c0 + 3] = g
+                heapq.heappush(heap, (float(t_in), (xi * ny + yi) * nz + zi))
     return gains, (act * np.float32(1000.0)).astype(np.float32)
 
 
@@ -396,7 +418,9 @@ def _ap_params(types, numbers, positions, spec: ScenarioSpec, current_factor) ->
     gains, act_ms = _connect_voxels(types, numbers, positions, spec.velocity_m_per_s, current_factor)
     samples = _delay_samples(types, numbers, positions, spec.velocity_m_per_s, spec.sample_rate_hz)
     delays = samples.astype(np.int64).astype(np.int32)  # from_samples_to_usize truncates
-    coefs = np.vectorize(from_samples_to_coef, otypes=[np.float32])(samples).astype(np.float32)
+    frac = np.fmod(samples.astype(np.float32), np.float32(1.0))
+    coefs = ((np.float32(1.0) - frac) / (np.float32(1.0) + frac)).astype(np.float32)
+    coefs = np.clip(coefs, np.float32(1e-4), np.float32(1.0) - np.float32(1e-4)).astype(np.float32)
     osi = _output_state_indices(types, numbers)
     return APParams(
         gains=gains,
