@@ -75,6 +75,11 @@ EXPORTED = [
     "ct_scenario_dims",
     "ct_run_epoch",
     "ct_run_epoch_plain",
+    "ct_batch_create",
+    "ct_batch_destroy",
+    "ct_batch_run_epoch",
+    "ct_batch_sync",
+    "ct_batch_info",
     "ct_simulate",
     "ct_set_algorithm",
     "ct_set_freeze",
@@ -159,6 +164,11 @@ def load(path: pathlib.Path = LIB_PATH) -> ctypes.CDLL:
     lib.ct_scenario_dims.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int64)] * 4
     lib.ct_run_epoch.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), _ip, ctypes.c_int, ctypes.c_int]
     lib.ct_run_epoch_plain.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), _ip]
+    lib.ct_batch_create.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    lib.ct_batch_destroy.argtypes = [vp]
+    lib.ct_batch_run_epoch.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    lib.ct_batch_sync.argtypes = [vp]
+    lib.ct_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int)]
     lib.ct_simulate.argtypes = [vp, _fp, _fp]
     lib.ct_set_algorithm.argtypes = [vp, ctypes.POINTER(CtAlgorithm)]
     lib.ct_set_freeze.argtypes = [vp, ctypes.c_int, ctypes.c_int]

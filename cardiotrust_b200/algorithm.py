@@ -309,6 +309,53 @@ class Data:
     measurements: np.ndarray
 
 
+class EpochBatch:
+    """Several :class:`EpochEngine` scenarios of one context run as one schedule per epoch.
+
+    Per beat index, one persistent forward launch and (adjoint mode) one
+    persistent adjoint launch cover the tiles of every member; the epoch is
+    captured once as a CUDA graph and replayed. Members need batch_size 0;
+    their beats run in index order. Destroy the batch before its members.
+    """
+
+    def __init__(self, ctx: "Context", engines, grad_mode=GradMode.Reference, precision=Precision.Fp32):
+        self._ctx = ctx
+        self._engines = list(engines)
+        handles = (ctypes.c_void_p * len(self._engines))(*[e._h.value for e in self._engines])
+        h = ctypes.c_void_p()
+        check(lib().ct_batch_create(ctx.handle, handles, len(self._engines), int(grad_mode), int(precision),
+                                    ctypes.byref(h)))
+        self._h = h
+        self.batch_indices = np.zeros(len(self._engines), dtype=np.int64)
+
+    def run_epoch(self, sync: bool = True) -> np.ndarray:
+        """One epoch of every member; returns the members' batch indices afterwards."""
+        check(lib().ct_batch_run_epoch(self._h, self.batch_indices.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        if sync:
+            self.sync()
+        return self.batch_indices.copy()
+
+    def sync(self) -> None:
+        check(lib().ct_batch_sync(self._h))
+
+    def info(self) -> dict:
+        k = ctypes.c_int64()
+        g = ctypes.c_int()
+        check(lib().ct_batch_info(self._h, ctypes.byref(k), ctypes.byref(g)))
+        return {"graph_kernels": int(k.value), "uses_graph": bool(g.value)}
+
+    def close(self) -> None:
+        if self._h:
+            lib().ct_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Results:
     """``Results`` (results.rs:28-34) whose arrays live on the GPU; attribute groups read on access."""
 

@@ -52,6 +52,14 @@ struct ct_scn {
   // +1 per update that rolls delays (roll_delays moves a delay by at most one). Sizes the
   // adjoint ring without reading the device.
   int64_t dmax_bound = 1;
+  // Asynchronous read-back of the device's largest delay after an update (pinned word + event):
+  // once it has landed, the bound becomes that value plus the updates enqueued since.
+  int32_t* dmax_host = nullptr;
+  cudaEvent_t dmax_event = nullptr;
+  int64_t updates = 0;          // updates that may roll delays, enqueued so far
+  int64_t updates_at_read = -1; // `updates` when the pending read-back was enqueued (-1: none)
+  // bumped whenever the algorithm settings change (batches re-capture their epoch graph)
+  uint64_t config_gen = 0;
   // Device voxel order: device voxel u holds reference voxel perm[u]; inv is the inverse.
   std::vector<int32_t> perm, inv;
   // launch accounting and optional per-phase CUDA-event timing
@@ -170,6 +178,36 @@ void release(ct_scn* s, void* p) {
   s->allocations.erase(std::remove(s->allocations.begin(), s->allocations.end(), p), s->allocations.end());
 }
 
+// After an update that may roll delays: count it and enqueue the read-back of the largest delay.
+void note_delay_update(ct_scn* s, cudaStream_t st) {
+  s->updates += 1;
+  s->dmax_bound = std::min<int64_t>(s->dmax_bound + 1, 1000);
+  if (!s->dmax_host) {
+    void* p = nullptr;
+    if (cudaMallocHost(&p, sizeof(int32_t)) != cudaSuccess) return;
+    if (cudaEventCreateWithFlags(&s->dmax_event, cudaEventDisableTiming) != cudaSuccess) {
+      cudaFreeHost(p);
+      return;
+    }
+    s->dmax_host = static_cast<int32_t*>(p);
+  }
+  if (s->updates_at_read >= 0 && cudaEventQuery(s->dmax_event) != cudaSuccess) return;  // one in flight
+  if (cudaMemcpyAsync(s->dmax_host, s->d.dmin + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaEventRecord(s->dmax_event, st) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  s->updates_at_read = s->updates;
+}
+
+// Tightens dmax_bound with a read-back that has landed.
+void refresh_delay_bound(ct_scn* s) {
+  if (s->updates_at_read < 0 || cudaEventQuery(s->dmax_event) != cudaSuccess) return;
+  const int64_t bound = std::max<int64_t>(1, *s->dmax_host) + (s->updates - s->updates_at_read);
+  s->dmax_bound = std::min<int64_t>(s->dmax_bound, bound);
+  s->updates_at_read = -1;
+}
+
 // Adjoint-mode buffers, allocated on first use; the ring grows with the delay bound.
 int prepare_adjoint(ct_scn* s) {
   DeviceScenario& d = s->d;
@@ -189,10 +227,11 @@ int prepare_adjoint(ct_scn* s) {
       }
     const int64_t nseg = (d.T + ct::kCkptSteps - 1) / ct::kCkptSteps;
     const int64_t seg_steps = std::min<int64_t>(d.T, ct::kCkptSteps);
+    d.adj_pitch = (int)(((plane + 3) / 4) * 4);
     int rc = alloc(s, &d.rev, V * kOffsets);
     if (!rc) rc = alloc(s, &d.ckpt, nseg * plane);
-    if (!rc) rc = alloc(s, &d.seg_ap, seg_steps * plane);
-    if (!rc) rc = alloc(s, &d.seg_q, seg_steps * plane);
+    if (!rc) rc = alloc(s, &d.seg_ap, seg_steps * d.adj_pitch);
+    if (!rc) rc = alloc(s, &d.seg_q, seg_steps * d.adj_pitch);
     if (!rc) rc = alloc(s, &d.dCk, plane);
     if (rc) {
       for (void* p : {(void*)d.rev, (void*)d.ckpt, (void*)d.seg_ap, (void*)d.seg_q, (void*)d.dCk}) release(s, p);
@@ -208,14 +247,19 @@ int prepare_adjoint(ct_scn* s) {
     d.adj_grid = (int)std::min<int64_t>((V + ct::kFwdTileVoxels - 1) / ct::kFwdTileVoxels,
                                         ct::adjoint_capacity(s->ctx->device));
   }
+  if (!d.lam_state) {
+    int rc = alloc(s, &d.lam_state, plane);
+    if (rc) return rc;
+  }
+  refresh_delay_bound(s);
   int need = 1;
   while (need < s->dmax_bound + ct::kMaxStepBlock + 2) need <<= 1;
-  if (!d.lam || d.adj_ring < need) {
-    CT_CUDA(cudaStreamSynchronize(st), "adjoint ring");
-    release(s, d.lam);
-    d.lam = nullptr;
+  if (!d.inbox || d.adj_ring < need) {
+    CT_CUDA(cudaStreamSynchronize(st), "adjoint inbox");
+    release(s, d.inbox);
+    d.inbox = nullptr;
     d.adj_ring = 0;
-    int rc = alloc(s, &d.lam, (int64_t)need * plane);
+    int rc = alloc(s, &d.inbox, (int64_t)need * d.adj_pitch);
     if (rc) return rc;
     d.adj_ring = need;
   }
@@ -319,7 +363,7 @@ int batch_end(ct_scn* s, int64_t n_beats, int64_t* batch_index) {
   return ct::launch_batch_metrics(d, *batch_index, st);
   });
   if (err != cudaSuccess) return cuda_fail(err, "update kernels");
-  if (!a.freeze_delays) s->dmax_bound = std::min<int64_t>(s->dmax_bound + 1, 1000);
+  if (!a.freeze_delays) note_delay_update(s, st);
   s->adam_step += 1;
   *batch_index += 1;
   return CT_OK;
@@ -514,6 +558,10 @@ void free_scenario(ct_scn* s) {
   s->pending.clear();
   for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
   s->event_pool.clear();
+  if (s->dmax_host) cudaFreeHost(s->dmax_host);
+  if (s->dmax_event) cudaEventDestroy(s->dmax_event);
+  s->dmax_host = nullptr;
+  s->dmax_event = nullptr;
 }
 
 int field_bytes(const ct_scn* s, int field, size_t* nbytes) {
@@ -992,6 +1040,7 @@ int ct_set_algorithm(ct_scn* scn, const ct_algorithm* algo) {
   int rc = check_algo(algo);
   if (rc) return rc;
   scn->algo = *algo;
+  scn->config_gen += 1;
   return CT_OK;
 }
 
@@ -999,12 +1048,14 @@ int ct_set_freeze(ct_scn* scn, int freeze_gains, int freeze_delays) {
   if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
   scn->algo.freeze_gains = freeze_gains != 0;
   scn->algo.freeze_delays = freeze_delays != 0;
+  scn->config_gen += 1;
   return CT_OK;
 }
 
 int ct_set_learning_rate(ct_scn* scn, float learning_rate) {
   if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
   scn->algo.learning_rate = learning_rate;
+  scn->config_gen += 1;
   return CT_OK;
 }
 
@@ -1084,6 +1135,7 @@ int ct_write_field(ct_scn* scn, int field, const void* src, size_t nbytes) {
           return fail(CT_ERR_INVALID_ARGUMENT, "delay %zu of a connected pair is %d; delays must be >= 1", i, del[i]);
       dst = d.delays;
       scn->dmax_bound = max_connected_delay(nbr, del);
+      scn->updates_at_read = -1;
       break;
     }
     case CT_FIELD_MEASUREMENTS_ACTUAL: dst = d.meas; break;
@@ -1163,6 +1215,470 @@ int ct_read_profile(ct_scn* scn, double* ms, int64_t* launches) {
     ms[i] = scn->phase_ms[i];
     launches[i] = scn->phase_launches[i];
   }
+  return CT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- batched scenarios
+//
+// A batch runs one epoch of every member scenario as one schedule: per beat
+// index b, one cooperative forward launch over the tiles of every scenario
+// that has a beat b, the measurement products of each scenario on parallel
+// streams, then one cooperative adjoint launch (or the per-scenario reference
+// derivations), the step metrics, and finally every scenario's update. The
+// whole epoch is captured once as a CUDA graph and replayed; the values that
+// change from epoch to epoch (Adam bias corrections, batch-metric slots) are
+// read by the kernels from a small device array written before each replay.
+
+struct EpochDev {
+  float bias[2];        // 1 - beta1^step, 1 - beta2^step (host powf, as in update.rs:140-141)
+  int64_t batch_index;  // batch-wise metric slot
+};
+
+struct ct_batch {
+  ct_ctx* ctx = nullptr;
+  std::vector<ct_scn*> scns;
+  int grad_mode = CT_GRAD_REFERENCE;
+  int precision = CT_PREC_FP32;
+  int nbeats_max = 0;
+  int fwd_grid = 0, adj_grid = 0;
+  std::vector<std::vector<int2>> beat_tiles;  // per beat index: tiles of the scenarios with that beat
+  std::vector<int> beat_tmax;
+  std::vector<int2*> beat_tiles_dev;
+  std::vector<float*> parts;                  // per scenario [T, tiles] step partials
+  std::vector<int> ntiles;
+  ct::FwdArgs* fwd_dev = nullptr;
+  ct::AdjScn* adj_dev = nullptr;
+  EpochDev* epoch_dev = nullptr;
+  std::vector<void*> allocations;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> fork_ev, join_ev;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool use_graph = true;
+  std::vector<int> captured_ring;
+  std::vector<uint64_t> captured_gen;
+  int64_t graph_kernels = 0;
+};
+
+namespace {
+
+int batch_alloc(ct_batch* b, void** p, size_t bytes) {
+  cudaError_t err = cudaMalloc(p, bytes > 0 ? bytes : 1);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc (batch)");
+  b->allocations.push_back(*p);
+  return CT_OK;
+}
+
+void batch_free(ct_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  for (void* p : b->allocations) cudaFree(p);
+  b->allocations.clear();
+  for (cudaStream_t s : b->side) cudaStreamDestroy(s);
+  for (cudaEvent_t e : b->fork_ev) cudaEventDestroy(e);
+  for (cudaEvent_t e : b->join_ev) cudaEventDestroy(e);
+  b->side.clear();
+  b->fork_ev.clear();
+  b->join_ev.clear();
+}
+
+// Fork every side stream off the main stream / join them back (event record + wait; captured as graph edges).
+cudaError_t fork_side(ct_batch* b) {
+  cudaStream_t st = b->ctx->stream;
+  for (size_t i = 0; i < b->side.size(); ++i) {
+    cudaError_t e = cudaEventRecord(b->fork_ev[i], st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side[i], b->fork_ev[i], 0);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+cudaError_t join_side(ct_batch* b) {
+  cudaStream_t st = b->ctx->stream;
+  for (size_t i = 0; i < b->side.size(); ++i) {
+    cudaError_t e = cudaEventRecord(b->join_ev[i], b->side[i]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->join_ev[i], 0);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+#define B_CUDA(expr)                         \
+  do {                                       \
+    cudaError_t e__ = (expr);                \
+    if (e__ != cudaSuccess) return e__;      \
+  } while (0)
+
+// Everything of one epoch, enqueued on the context stream and the side streams.
+cudaError_t batch_enqueue_epoch(ct_batch* b) {
+  cudaStream_t st = b->ctx->stream;
+  const size_t n = b->scns.size();
+  auto side_of = [&](size_t i) { return b->side[i % b->side.size()]; };
+  const bool adjoint = b->grad_mode == CT_GRAD_ADJOINT;
+  // Derivatives::reset of every scenario
+  B_CUDA(fork_side(b));
+  for (size_t i = 0; i < n; ++i) {
+    DeviceScenario& d = b->scns[i]->d;
+    cudaStream_t s = side_of(i);
+    B_CUDA(cudaMemsetAsync(d.dG, 0, sizeof(float) * d.S * kGainCols, s));
+    B_CUDA(cudaMemsetAsync(d.dC, 0, sizeof(float) * d.V * kOffsets, s));
+    B_CUDA(cudaMemsetAsync(d.fir, 0, sizeof(float) * d.V * kGainCols, s));
+    B_CUDA(cudaMemsetAsync(d.iir, 0, sizeof(float) * d.V * kGainCols, s));
+    B_CUDA(cudaMemsetAsync(d.mreg_sum, 0, sizeof(float), s));
+  }
+  B_CUDA(join_side(b));
+  for (int beat = 0; beat < b->nbeats_max; ++beat) {
+    // forward of every scenario with this beat
+    B_CUDA(fork_side(b));
+    for (size_t i = 0; i < n; ++i) {
+      DeviceScenario& d = b->scns[i]->d;
+      if (beat >= d.B) continue;
+      B_CUDA(cudaMemsetAsync(d.ap, 0, sizeof(float) * d.V * kGainCols, side_of(i)));
+      B_CUDA(cudaMemsetAsync(d.ap_last, 0, sizeof(float) * d.V * kGainCols, side_of(i)));
+      if (adjoint) {
+        B_CUDA(cudaMemsetAsync(d.inbox, 0, sizeof(float) * d.adj_ring * (size_t)d.adj_pitch, side_of(i)));
+        B_CUDA(cudaMemsetAsync(d.lam_state, 0, sizeof(float) * d.V * kGainCols, side_of(i)));
+      }
+    }
+    B_CUDA(join_side(b));
+    DeviceScenario& d0 = b->scns[0]->d;
+    ct::FwdBatch fb;
+    fb.scns = b->fwd_dev;
+    fb.nscn = (int)n;
+    fb.tiles = b->beat_tiles_dev[(size_t)beat];
+    fb.ntiles = (int)b->beat_tiles[(size_t)beat].size();
+    fb.Tmax = b->beat_tmax[(size_t)beat];
+    fb.status = d0.status;
+    fb.barrier = d0.barrier;
+    B_CUDA(ct::launch_forward_batch(fb, std::min(b->fwd_grid, fb.ntiles), st));
+    // measurement products, residuals, (reference) derivations and step metrics per scenario
+    B_CUDA(fork_side(b));
+    for (size_t i = 0; i < n; ++i) {
+      ct_scn* s = b->scns[i];
+      DeviceScenario& d = s->d;
+      if (beat >= d.B) continue;
+      cudaStream_t ss = side_of(i);
+      const ct_algorithm& a = s->algo;
+      if (b->precision == CT_PREC_FP32) {
+        B_CUDA(ct::launch_measure(d, beat, true, ss));
+        B_CUDA(ct::launch_map_residuals(d, beat, ss));
+      } else {
+        B_CUDA(ct::launch_measure_umma(d, beat, true, b->precision, ss));
+        B_CUDA(ct::launch_map_residuals_umma(d, beat, b->precision, ss));
+      }
+      if (!adjoint && (!a.freeze_gains || !a.freeze_delays)) {
+        ct::DeriveScalars ds;
+        ds.mse_scaling = 1.0f / (float)d.M * a.mse_strength;
+        ds.reg_scaling = a.maximum_regularization_strength;
+        ds.threshold = a.maximum_regularization_threshold;
+        ds.diffreg = a.difference_regularization_strength;
+        ds.freeze_gains = a.freeze_gains;
+        ds.freeze_delays = a.freeze_delays;
+        ds.ap_derivative = a.ap_derivative;
+        B_CUDA(ct::launch_derive(d, ds, ss));
+      }
+      B_CUDA(ct::launch_step_metrics_parts(d, b->parts[i], b->ntiles[i], a.maximum_regularization_strength, ss));
+    }
+    B_CUDA(join_side(b));
+    if (adjoint) {
+      ct::AdjLaunch al;
+      al.scns = b->adj_dev;
+      al.nscn = (int)n;
+      al.tiles = fb.tiles;
+      al.ntiles = fb.ntiles;
+      al.Tmax = fb.Tmax;
+      al.ckpt_steps = ct::kCkptSteps;
+      al.status = d0.status;
+      al.barrier = d0.barrier;
+      B_CUDA(ct::launch_adjoint_tiles(al, std::min(b->adj_grid, fb.ntiles), st));
+    }
+  }
+  // calculate_average_delays -> batch derivatives -> update -> batch metrics, per scenario
+  B_CUDA(fork_side(b));
+  for (size_t i = 0; i < n; ++i) {
+    ct_scn* s = b->scns[i];
+    DeviceScenario& d = s->d;
+    const ct_algorithm& a = s->algo;
+    cudaStream_t ss = side_of(i);
+    B_CUDA(ct::launch_average_delays(d, ss));
+    if (!a.freeze_delays && std::fabs(a.smoothness_regularization_strength) > 1.1920929e-7f)
+      B_CUDA(ct::launch_smoothness(d, a.smoothness_regularization_strength, ss));
+    ct::UpdateScalars u;
+    u.optimizer = a.optimizer;
+    u.freeze_gains = a.freeze_gains;
+    u.freeze_delays = a.freeze_delays;
+    u.lr_over_bs = a.learning_rate / (float)(d.T * d.B);
+    u.bias1 = u.bias2 = 1.0f;
+    u.bias_dev = b->epoch_dev[i].bias;
+    B_CUDA(ct::launch_update(d, u, ss));
+    if (!a.freeze_delays) B_CUDA(ct::launch_min_delay(d, ss));
+    B_CUDA(ct::launch_batch_metrics_dev(d, &b->epoch_dev[i].batch_index, ss));
+  }
+  B_CUDA(join_side(b));
+  return cudaSuccess;
+}
+
+// (Re)builds the per-scenario device descriptors and, if possible, the epoch graph.
+int batch_prepare(ct_batch* b) {
+  cudaStream_t st = b->ctx->stream;
+  const size_t n = b->scns.size();
+  bool stale = b->exec == nullptr && b->use_graph;
+  for (size_t i = 0; i < n; ++i) {
+    ct_scn* s = b->scns[i];
+    if (b->grad_mode == CT_GRAD_ADJOINT) {
+      const int before = s->d.adj_ring;
+      int rc = prepare_adjoint(s);
+      if (rc) return rc;
+      if (s->d.adj_ring != before) stale = true;
+    }
+    if (b->captured_ring.size() == n && b->captured_ring[i] != s->d.adj_ring) stale = true;
+    if (b->captured_gen.size() == n && b->captured_gen[i] != s->config_gen) stale = true;
+  }
+  if (!stale && b->captured_ring.size() == n) return CT_OK;
+  // descriptors
+  std::vector<ct::FwdArgs> fa(n);
+  std::vector<ct::AdjScn> aa(n);
+  for (size_t i = 0; i < n; ++i) {
+    ct_scn* s = b->scns[i];
+    const ct_algorithm& a = s->algo;
+    DeviceScenario& d = s->d;
+    const bool adjoint = b->grad_mode == CT_GRAD_ADJOINT && (!a.freeze_gains || !a.freeze_delays);
+    fa[i] = ct::forward_scenario(d, a.maximum_regularization_threshold, adjoint ? d.ckpt : nullptr, b->parts[i],
+                                 b->ntiles[i]);
+    ct::AdjointScalars as;
+    as.mse_scaling = 1.0f / (float)d.M * a.mse_strength;
+    as.reg_scaling = a.maximum_regularization_strength;
+    as.threshold = a.maximum_regularization_threshold;
+    as.diffreg = a.difference_regularization_strength;
+    as.freeze_gains = a.freeze_gains || !adjoint;
+    as.freeze_delays = a.freeze_delays || !adjoint;
+    as.ap_derivative = a.ap_derivative;
+    aa[i] = b->grad_mode == CT_GRAD_ADJOINT ? ct::adjoint_scenario(d, as) : ct::AdjScn{};
+  }
+  CT_CUDA(cudaMemcpyAsync(b->fwd_dev, fa.data(), sizeof(ct::FwdArgs) * n, cudaMemcpyHostToDevice, st), "batch upload");
+  if (b->grad_mode == CT_GRAD_ADJOINT)
+    CT_CUDA(cudaMemcpyAsync(b->adj_dev, aa.data(), sizeof(ct::AdjScn) * n, cudaMemcpyHostToDevice, st),
+            "batch upload");
+  CT_CUDA(cudaStreamSynchronize(st), "batch upload");
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->graph_kernels = 0;
+  if (b->use_graph) {
+    cudaError_t err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+      cudaError_t body = batch_enqueue_epoch(b);
+      cudaGraph_t g = nullptr;
+      err = cudaStreamEndCapture(st, &g);
+      if (body == cudaSuccess && err == cudaSuccess && g) {
+        err = cudaGraphInstantiate(&b->exec, g, 0);
+        b->graph = g;
+        if (err == cudaSuccess) {
+          size_t count = 0;
+          cudaGraphGetNodes(g, nullptr, &count);
+          std::vector<cudaGraphNode_t> nodes(count);
+          cudaGraphGetNodes(g, nodes.data(), &count);
+          for (cudaGraphNode_t nd : nodes) {
+            cudaGraphNodeType ty;
+            if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++b->graph_kernels;
+          }
+        }
+      } else if (g) {
+        cudaGraphDestroy(g);
+      }
+      if (body != cudaSuccess || err != cudaSuccess || !b->exec) {
+        // capture refused (e.g. a driver without cooperative graph nodes): run the same schedule eagerly
+        cudaGetLastError();
+        if (b->exec) cudaGraphExecDestroy(b->exec);
+        if (b->graph) cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+        b->use_graph = false;
+      }
+    } else {
+      cudaGetLastError();
+      b->use_graph = false;
+    }
+  }
+  b->captured_ring.assign(n, 0);
+  b->captured_gen.assign(n, 0);
+  for (size_t i = 0; i < n; ++i) {
+    b->captured_ring[i] = b->scns[i]->d.adj_ring;
+    b->captured_gen[i] = b->scns[i]->config_gen;
+  }
+  return CT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ct_batch_create(ct_ctx* ctx, ct_scn* const* scenarios, int64_t count, int grad_mode, int precision,
+                    ct_batch** out) {
+  if (!ctx || !scenarios || !out || count <= 0) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument or empty batch");
+  *out = nullptr;
+  if (grad_mode != CT_GRAD_REFERENCE && grad_mode != CT_GRAD_ADJOINT)
+    return fail(CT_ERR_NOT_SUPPORTED, "gradient mode %d", grad_mode);
+  if (precision != CT_PREC_FP32 && precision != CT_PREC_TF32X3 && precision != CT_PREC_TF32)
+    return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
+  for (int64_t i = 0; i < count; ++i) {
+    ct_scn* s = scenarios[i];
+    if (!s) return fail(CT_ERR_INVALID_ARGUMENT, "scenario %lld is NULL", (long long)i);
+    if (s->ctx != ctx) return fail(CT_ERR_INVALID_ARGUMENT, "scenario %lld belongs to another context", (long long)i);
+    if (s->algo.batch_size != 0)
+      return fail(CT_ERR_NOT_SUPPORTED, "scenario %lld: batches need batch_size 0 (one update per epoch)",
+                  (long long)i);
+    if (precision != CT_PREC_FP32 && !s->d.umma)
+      return fail(CT_ERR_NOT_SUPPORTED, "scenario %lld: tensor-core precision needs num_states divisible by 4",
+                  (long long)i);
+    for (int64_t j = 0; j < i; ++j)
+      if (scenarios[j] == s) return fail(CT_ERR_INVALID_ARGUMENT, "scenario %lld appears twice", (long long)i);
+  }
+  CT_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  ct_batch* b = new ct_batch;
+  b->ctx = ctx;
+  b->grad_mode = grad_mode;
+  b->precision = precision;
+  b->scns.assign(scenarios, scenarios + count);
+  const size_t n = b->scns.size();
+  int rc = CT_OK;
+  // tiles: scenarios by decreasing beat length, so that at any step the live tiles form a prefix of the
+  // list, which the round-robin tile -> CTA assignment spreads evenly
+  std::vector<size_t> order(n);
+  for (size_t i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return b->scns[x]->d.T > b->scns[y]->d.T; });
+  b->ntiles.resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    DeviceScenario& d = b->scns[i]->d;
+    b->ntiles[i] = (int)((d.V + ct::kFwdTileVoxels - 1) / ct::kFwdTileVoxels);
+    b->nbeats_max = std::max<int>(b->nbeats_max, (int)d.B);
+  }
+  b->beat_tiles.resize((size_t)b->nbeats_max);
+  b->beat_tmax.assign((size_t)b->nbeats_max, 0);
+  for (int beat = 0; beat < b->nbeats_max; ++beat)
+    for (size_t i : order) {
+      DeviceScenario& d = b->scns[i]->d;
+      if (beat >= d.B) continue;
+      b->beat_tmax[(size_t)beat] = std::max<int>(b->beat_tmax[(size_t)beat], (int)d.T);
+      for (int t = 0; t < b->ntiles[i]; ++t)
+        b->beat_tiles[(size_t)beat].push_back(make_int2((int)i, t * ct::kFwdTileVoxels));
+    }
+  b->fwd_grid = ct::forward_batch_capacity(ctx->device);
+  b->adj_grid = ct::adjoint_capacity(ctx->device);
+  void* p = nullptr;
+  rc = batch_alloc(b, &p, sizeof(ct::FwdArgs) * n);
+  b->fwd_dev = static_cast<ct::FwdArgs*>(p);
+  if (!rc) {
+    rc = batch_alloc(b, &p, sizeof(ct::AdjScn) * n);
+    b->adj_dev = static_cast<ct::AdjScn*>(p);
+  }
+  if (!rc) {
+    rc = batch_alloc(b, &p, sizeof(EpochDev) * n);
+    b->epoch_dev = static_cast<EpochDev*>(p);
+  }
+  for (size_t i = 0; i < n && !rc; ++i) {
+    DeviceScenario& d = b->scns[i]->d;
+    rc = batch_alloc(b, &p, sizeof(float) * (size_t)d.T * b->ntiles[i]);
+    b->parts.push_back(static_cast<float*>(p));
+  }
+  for (int beat = 0; beat < b->nbeats_max && !rc; ++beat) {
+    const auto& tl = b->beat_tiles[(size_t)beat];
+    rc = batch_alloc(b, &p, sizeof(int2) * tl.size());
+    b->beat_tiles_dev.push_back(static_cast<int2*>(p));
+    if (!rc) {
+      cudaError_t e = cudaMemcpy(p, tl.data(), sizeof(int2) * tl.size(), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) rc = cuda_fail(e, "batch tiles");
+    }
+  }
+  const int nside = (int)std::min<size_t>(n, 8);
+  for (int i = 0; i < nside && !rc; ++i) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t e1 = nullptr, e2 = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&e1, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&e2, cudaEventDisableTiming);
+    if (e != cudaSuccess) rc = cuda_fail(e, "batch streams");
+    if (s) b->side.push_back(s);
+    if (e1) b->fork_ev.push_back(e1);
+    if (e2) b->join_ev.push_back(e2);
+  }
+  if (rc) {
+    batch_free(b);
+    delete b;
+    return rc;
+  }
+  ctx->refs += 1;
+  *out = b;
+  return CT_OK;
+}
+
+int ct_batch_destroy(ct_batch* b) {
+  if (!b) return CT_OK;
+  ct_ctx* ctx = b->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  batch_free(b);
+  delete b;
+  ctx_release(ctx);
+  return CT_OK;
+}
+
+int ct_batch_run_epoch(ct_batch* b, int64_t* batch_indices) {
+  if (!b || !batch_indices) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  CT_CUDA(cudaSetDevice(b->ctx->device), "cudaSetDevice");
+  const size_t n = b->scns.size();
+  for (size_t i = 0; i < n; ++i) {
+    ct_scn* s = b->scns[i];
+    if (s->algo.batch_size != 0)
+      return fail(CT_ERR_NOT_SUPPORTED, "scenario %zu: batches need batch_size 0 (one update per epoch)", i);
+    if (batch_indices[i] < 0 || batch_indices[i] >= s->d.NB)
+      return fail(CT_ERR_BATCH_INDEX, "scenario %zu: batch index %lld outside the %lld batch-wise metric slots", i,
+                  (long long)batch_indices[i], (long long)s->d.NB);
+  }
+  int rc = batch_prepare(b);
+  if (rc) return rc;
+  std::vector<EpochDev> ep(n);
+  for (size_t i = 0; i < n; ++i) {
+    ct_scn* s = b->scns[i];
+    ep[i].bias[0] = 1.0f - powf(0.9f, (float)s->adam_step);
+    ep[i].bias[1] = 1.0f - powf(0.999f, (float)s->adam_step);
+    ep[i].batch_index = batch_indices[i];
+  }
+  cudaStream_t st = b->ctx->stream;
+  // pageable source: the copy is staged before the call returns, so `ep` may go out of scope
+  CT_CUDA(cudaMemcpyAsync(b->epoch_dev, ep.data(), sizeof(EpochDev) * n, cudaMemcpyHostToDevice, st),
+          "batch epoch scalars");
+  if (b->exec) {
+    CT_CUDA(cudaGraphLaunch(b->exec, st), "cudaGraphLaunch");
+  } else {
+    CT_CUDA(batch_enqueue_epoch(b), "batch epoch");
+  }
+  for (size_t i = 0; i < n; ++i) {
+    ct_scn* s = b->scns[i];
+    s->adam_step += 1;
+    batch_indices[i] += 1;
+    if (!s->algo.freeze_delays) note_delay_update(s, st);
+  }
+  return CT_OK;
+}
+
+int ct_batch_sync(ct_batch* b) {
+  if (!b) return fail(CT_ERR_INVALID_ARGUMENT, "batch is NULL");
+  for (ct_scn* s : b->scns) {
+    int rc = ct_sync(s);
+    if (rc) return rc;
+  }
+  return CT_OK;
+}
+
+int ct_batch_info(ct_batch* b, int64_t* graph_kernels, int* uses_graph) {
+  if (!b) return fail(CT_ERR_INVALID_ARGUMENT, "batch is NULL");
+  if (graph_kernels) *graph_kernels = b->graph_kernels;
+  if (uses_graph) *uses_graph = b->exec != nullptr ? 1 : 0;
   return CT_OK;
 }
 

@@ -76,9 +76,11 @@ struct DeviceScenario {
   float* ckpt;           // [ceil(T/kCkptSteps), V, 78] all-pass state before step s * kCkptSteps
   float* seg_ap;         // [kCkptSteps, V, 78] recomputed all-pass outputs of one segment
   float* seg_q;          // [kCkptSteps, V, 78] in_t - ap[t-1] of one segment
-  float* lam;            // [adj_ring, V, 78] adjoint all-pass values of recent steps
+  float* inbox;          // [adj_ring, V, 78] adjoint contributions addressed to (voxel, column) by step
+  float* lam_state;      // [V,78] adjoint all-pass state between blocks of steps
   float* dCk;            // [V,78] per-column coefficient-gradient partials
-  int adj_ring;          // ring slots (power of two)
+  int adj_ring;          // inbox slots (power of two)
+  int adj_pitch;         // floats per plane of seg_ap, seg_q and inbox: V * 78 rounded up to 4 (16-byte rows)
   int adj_grid;          // CTAs of the adjoint kernel
   // plain form (ct_plain.cu), allocated on first use
   float* plain_mreg;     // [S] maximum regularisation of the current step
@@ -91,6 +93,41 @@ struct DeviceScenario {
 int report_error(int status, const char* message);
 
 // ---- launchers (all enqueue on `stream`, return cudaError_t of the launch)
+
+// One scenario as the forward kernels see it.
+struct FwdArgs {
+  int V, S, T;
+  int part_stride;  // batched form: tiles of the scenario (stride of stepsum_part rows)
+  const int32_t* nbr;
+  const float* coefs;
+  const int32_t* delays;
+  const float* gains;
+  const float* ctrl;
+  const float* u;
+  float* X;
+  float* ap;
+  float* ap_last;
+  float* stepsum_part;
+  float* ckpt;  // adjoint checkpoints [ceil(T / kCkptSteps), V, 78] or null
+  const int32_t* dmin;
+  float threshold;
+  int32_t* status;
+  GridBarrier* barrier;
+};
+// One cooperative forward launch over the tiles of several scenarios (batched form).
+struct FwdBatch {
+  const FwdArgs* scns;  // device array
+  int nscn;
+  const int2* tiles;    // (scenario, first voxel)
+  int ntiles;
+  int Tmax;
+  int32_t* status;
+  GridBarrier* barrier;
+};
+FwdArgs forward_scenario(const DeviceScenario& d, float threshold, float* ckpt, float* part, int part_stride);
+// The caller zeroes every scenario's ap and ap_last first.
+cudaError_t launch_forward_batch(const FwdBatch& b, int grid, cudaStream_t stream);
+int forward_batch_capacity(int device);
 
 // Forward propagation of one beat: X[t,:] for t in [0,T). With ckpt non-null the all-pass
 // state before every step s * kCkptSteps (s >= 1) is stored in ckpt[s].
@@ -126,8 +163,46 @@ struct AdjointScalars {
   float mse_scaling, reg_scaling, threshold, diffreg;
   int freeze_gains, freeze_delays, ap_derivative;
 };
+// One scenario as the adjoint kernel sees it (device pointers, sizes, scalars).
+struct AdjScn {
+  int V, S, T, ring;
+  int pitch;  // floats between consecutive planes of seg_ap, seg_q and inbox (V * 78 rounded up to 4)
+  const int32_t* nbr;
+  const float* coefs;
+  const int32_t* delays;
+  const float* init_delays;
+  const float* gains;
+  const float* X;
+  const float* MR;
+  const float* ckpt;
+  float* seg_ap;
+  float* seg_q;
+  float* inbox;
+  float* lam_state;
+  float* dG;
+  float* dC;
+  float* dCk;
+  const int32_t* dmin;
+  float mse_scaling, reg_scaling, threshold, diffreg;
+  int freeze_gains, freeze_delays, ap_derivative;
+};
+// One cooperative adjoint launch over the tiles of one or more scenarios.
+struct AdjLaunch {
+  const AdjScn* scns;  // device array of nscn scenarios, or null: `single` is the only one
+  AdjScn single;
+  int nscn;
+  const int2* tiles;  // (scenario, first voxel) per tile, or null: tiles of 32 voxels of scenario 0
+  int ntiles;
+  int Tmax;           // longest beat of the launch
+  int ckpt_steps;     // checkpoint interval (power of two)
+  int32_t* status;
+  GridBarrier* barrier;
+};
+AdjScn adjoint_scenario(const DeviceScenario& d, const AdjointScalars& s);
 // Back-propagation through time of one beat (needs X, MR and the forward's checkpoints): dG, dC.
 cudaError_t launch_adjoint(DeviceScenario& d, const AdjointScalars& s, cudaStream_t stream);
+// The same over a tile list; the caller zeroes every scenario's inbox and lam_state first.
+cudaError_t launch_adjoint_tiles(const AdjLaunch& launch, int grid, cudaStream_t stream);
 // How many CTAs of the adjoint kernel fit on the device at once.
 int adjoint_capacity(int device);
 
@@ -141,8 +216,12 @@ int plain_step_launches(const PlainScalars& s);
 
 // Step metrics of one beat: loss_mr[t] (running), loss[t]; advances mreg_sum.
 cudaError_t launch_step_metrics(DeviceScenario& d, float reg_strength, cudaStream_t stream);
-// Batch metrics into slot `index`.
+// Batch metrics into slot `index`; the _dev form reads the slot on the device (graph replay).
 cudaError_t launch_batch_metrics(DeviceScenario& d, int64_t index, cudaStream_t stream);
+cudaError_t launch_batch_metrics_dev(DeviceScenario& d, const int64_t* index_dev, cudaStream_t stream);
+// Step metrics from `parts` per-step partial sums (the batched forward's per-tile partials).
+cudaError_t launch_step_metrics_parts(DeviceScenario& d, const float* part, int parts, float reg_strength,
+                                      cudaStream_t stream);
 
 cudaError_t launch_average_delays(DeviceScenario& d, cudaStream_t stream);
 cudaError_t launch_smoothness(DeviceScenario& d, float strength, cudaStream_t stream);
@@ -150,6 +229,7 @@ cudaError_t launch_smoothness(DeviceScenario& d, float strength, cudaStream_t st
 struct UpdateScalars {
   int optimizer, freeze_gains, freeze_delays;
   float lr_over_bs, bias1, bias2;
+  const float* bias_dev = nullptr;  // if set: {bias1, bias2} read on the device (graph replay)
 };
 cudaError_t launch_update(DeviceScenario& d, const UpdateScalars& s, cudaStream_t stream);
 cudaError_t launch_min_delay(DeviceScenario& d, cudaStream_t stream);

@@ -54,25 +54,6 @@ constexpr int kThreads = kProducers + kConsumers;
 constexpr int kBarFull = 1;   // named barriers kBarFull + buffer, kBarEmpty + buffer
 constexpr int kBarEmpty = 3;
 
-struct FwdArgs {
-  int V, S, T;
-  const int32_t* nbr;
-  const float* coefs;
-  const int32_t* delays;
-  const float* gains;
-  const float* ctrl;
-  const float* u;
-  float* X;
-  float* ap;
-  float* ap_last;
-  float* stepsum_part;
-  float* ckpt;  // adjoint checkpoints [ceil(T / kCkptSteps), V, 78] or null
-  const int32_t* dmin;
-  float threshold;
-  int32_t* status;
-  GridBarrier* barrier;
-};
-
 struct Smem {
   float4 g[kGainCols][kTileVoxels];                  // gains of the voxel's three rows at column k
   float ap_out[2][kRound][kTileVoxels * kGainCols];  // round buffers
@@ -156,6 +137,16 @@ __device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int 
       for (int b = 0; b < 3; ++b) h[i][q][b] = ok ? row[b] : 0.0f;
     }
   }
+  // adjoint checkpoint inside this round: step index after which the state is stored, or -1
+  int ck_s = -1;
+  float* ck_row = nullptr;
+  if (p.ckpt) {
+    const int tc = ((tr0 + kCkptSteps) & ~(kCkptSteps - 1)) - 1;  // first step t >= tr0 with (t+1) % K == 0
+    if (tc < tr0 + R && tc + 1 < p.T) {
+      ck_s = tc - tr0;
+      ck_row = p.ckpt + (size_t)((tc + 1) / kCkptSteps) * p.V * kGainCols + (size_t)v0 * kGainCols;
+    }
+  }
 #pragma unroll
   for (int i = 0; i < kItemsPerProducer; ++i) {
     const int e = threadIdx.x + i * kProducers;
@@ -176,8 +167,7 @@ __device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int 
             a = fmaf(c, h[i][s + 1][b] - a, h[i][s][b]);
             out0[s * (kTileVoxels * kGainCols) + b] = a;
             if (tr0 + s == p.T - 2) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = a;
-            if (p.ckpt && ((tr0 + s + 1) & (kCkptSteps - 1)) == 0 && tr0 + s + 1 < p.T)
-              p.ckpt[((size_t)((tr0 + s + 1) / kCkptSteps) * p.V + v0 + vl) * kGainCols + 3 * n + b] = a;
+            if (s == ck_s) ck_row[vl * kGainCols + 3 * n + b] = a;
           }
         }
         st[b] = a;
@@ -294,6 +284,67 @@ __global__ void __launch_bounds__(kThreads, 1) forward_stream_kernel(FwdArgs p) 
 }
 
 
+// ---- batched form: the streaming schedule over the tiles of several scenarios
+//
+// Every tile names its scenario; all scenarios advance through the same
+// absolute steps (a scenario whose beat is shorter idles once it is done),
+// L = the smallest min(dmin, kMaxStepBlock) of any scenario. Each tile writes
+// its own per-step max-regularisation partial, stepsum_part[t * part_stride +
+// tile of the scenario], so the step metrics of every scenario sum the same
+// partials in the same order.
+__global__ void __launch_bounds__(kThreads, 1) forward_batch_kernel(FwdBatch B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+  __shared__ FwdArgs sp;
+  const bool producer = threadIdx.x < kProducers;
+  int Lmax = kMaxStepBlock;
+  for (int s = 0; s < B.nscn; ++s) {
+    int dmin = B.scns[s].dmin[0];
+    if (dmin < 1) dmin = 1;
+    if (dmin < Lmax) Lmax = dmin;
+  }
+  int cur = -1;
+  int round = 0;
+  unsigned int barrier_number = 0;
+  for (int t0 = 0; t0 < B.Tmax; t0 += Lmax) {
+    for (int tile = blockIdx.x; tile < B.ntiles; tile += gridDim.x) {
+      const int2 tl = B.tiles[tile];
+      __syncthreads();
+      if (tl.x != cur) {
+        if (threadIdx.x == 0) sp = B.scns[tl.x];
+        cur = tl.x;
+        __syncthreads();
+      }
+      if (t0 >= sp.T) continue;  // uniform per CTA
+      const int L = (sp.T - t0) < Lmax ? (sp.T - t0) : Lmax;
+      const int v0 = tl.y;
+      const int nv = min(kTileVoxels, sp.V - v0);
+      if (threadIdx.x < kMaxStepBlock) sm.part[threadIdx.x] = 0.0f;
+      stage_tile(sm, sp, v0);
+      for (int r0 = 0; r0 < L; r0 += kRound, ++round) {
+        const int R = (L - r0) < kRound ? (L - r0) : kRound;
+        const int buf = round & 1;
+        if (producer) {
+          if (round >= 2) named_sync(kBarEmpty + buf, kThreads);
+          produce(sm, sp, v0, nv, t0 + r0, R, buf);
+          named_arrive(kBarFull + buf, kThreads);
+        } else {
+          named_sync(kBarFull + buf, kThreads);
+          consume(sm, sp, v0, nv, t0 + r0, R, buf, r0);
+          named_arrive(kBarEmpty + buf, kThreads);
+        }
+      }
+      __syncthreads();
+      unstage_tile(sm, sp, v0);
+      if ((int)threadIdx.x < L)
+        sp.stepsum_part[(size_t)(t0 + threadIdx.x) * sp.part_stride + v0 / kTileVoxels] = sm.part[threadIdx.x];
+    }
+    if (t0 + Lmax < B.Tmax) {
+      if (!grid_barrier(B.barrier, barrier_number++, B.status)) return;
+    }
+  }
+}
+
 // ---- resident form: one tile per CTA for the whole launch, neighbour history in a shared ring
 //
 // Each tile's halo (the device voxels its 26-neighbourhoods touch, at most
@@ -353,7 +404,8 @@ __device__ __forceinline__ void stage_rows(RingSmem& sm, const FwdArgs& p, int n
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 1) forward_ring_kernel(FwdArgs p, RingArgs ra) {
+// Two CTAs per SM (<= 170 registers) keep up to 296 tiles co-resident.
+__global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, RingArgs ra) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RingSmem& sm = *reinterpret_cast<RingSmem*>(smem_raw);
   const int T = p.T, S = p.S;
@@ -443,6 +495,16 @@ __global__ void __launch_bounds__(kThreads, 1) forward_ring_kernel(FwdArgs p, Ri
           cp_async_commit();
         }
         if (round >= 2) named_sync(kBarEmpty + buf, kThreads);
+        // adjoint checkpoint inside this round: step index s2 after which the state is stored, or -1
+        int ck_s = -1;
+        float* ck_row = nullptr;
+        if (p.ckpt) {
+          const int tc = ((tr0 + kCkptSteps) & ~(kCkptSteps - 1)) - 1;  // first step t >= tr0 with (t+1) % K == 0
+          if (tc < tr0 + R && tc + 1 < T) {
+            ck_s = tc - tr0;
+            ck_row = p.ckpt + (size_t)((tc + 1) / kCkptSteps) * p.V * kGainCols + (size_t)v0 * kGainCols;
+          }
+        }
 #pragma unroll
         for (int i = 0; i < kItemsPerProducer; ++i) {
           const int e = threadIdx.x + i * kProducers;
@@ -475,8 +537,7 @@ __global__ void __launch_bounds__(kThreads, 1) forward_ring_kernel(FwdArgs p, Ri
                   a = fmaf(cc[i], h[s2 + 1][b] - a, h[s2][b]);
                   out0[s2 * (kTileVoxels * kGainCols) + b] = a;
                   if (tr0 + s2 == T - 2) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = a;
-                  if (p.ckpt && ((tr0 + s2 + 1) & (kCkptSteps - 1)) == 0 && tr0 + s2 + 1 < T)
-                    p.ckpt[((size_t)((tr0 + s2 + 1) / kCkptSteps) * p.V + v0 + vl) * kGainCols + 3 * n + b] = a;
+                  if (s2 == ck_s) ck_row[vl * kGainCols + 3 * n + b] = a;
                 }
               }
               st[i][b] = a;
@@ -574,19 +635,26 @@ int forward_grid_size(int64_t V, int device) {
   return (int)grid;
 }
 
-int forward_ring_capacity(int device) {
-  forward_grid_size(1, device);  // sets the shared-memory attributes
+int forward_batch_capacity(int device) {
+  forward_grid_size(1, device);
+  static bool configured[128] = {};
+  if (device >= 0 && device < 128 && !configured[device]) {
+    cudaFuncSetAttribute(forward_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+    configured[device] = true;
+  }
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, forward_ring_kernel, kThreads, sizeof(RingSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, forward_batch_kernel, kThreads, sizeof(Smem));
+  if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
 }
 
-cudaError_t launch_forward(DeviceScenario& d, float threshold, float* ckpt, cudaStream_t stream) {
+FwdArgs forward_scenario(const DeviceScenario& d, float threshold, float* ckpt, float* part, int part_stride) {
   FwdArgs a;
   a.V = (int)d.V;
   a.S = (int)d.S;
   a.T = (int)d.T;
+  a.part_stride = part_stride;
   a.nbr = d.nbr;
   a.coefs = d.coefs;
   a.delays = d.delays;
@@ -596,12 +664,34 @@ cudaError_t launch_forward(DeviceScenario& d, float threshold, float* ckpt, cuda
   a.X = d.X;
   a.ap = d.ap;
   a.ap_last = d.ap_last;
-  a.stepsum_part = d.stepsum_part;
+  a.stepsum_part = part;
   a.ckpt = ckpt;
   a.dmin = d.dmin;
   a.threshold = threshold;
   a.status = d.status;
   a.barrier = d.barrier;
+  return a;
+}
+
+cudaError_t launch_forward_batch(const FwdBatch& b, int grid, cudaStream_t stream) {
+  // forward_batch_capacity (called when the batch is made) has set the shared-memory attribute
+  cudaError_t err = cudaMemsetAsync(b.barrier, 0, sizeof(GridBarrier), stream);
+  if (err != cudaSuccess) return err;
+  FwdBatch l = b;
+  void* args[] = {&l};
+  return launch_cooperative((const void*)forward_batch_kernel, grid, kThreads, args, sizeof(Smem), stream);
+}
+
+int forward_ring_capacity(int device) {
+  forward_grid_size(1, device);  // sets the shared-memory attributes
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, forward_ring_kernel, kThreads, sizeof(RingSmem));
+  return sms * per_sm;
+}
+
+cudaError_t launch_forward(DeviceScenario& d, float threshold, float* ckpt, cudaStream_t stream) {
+  FwdArgs a = forward_scenario(d, threshold, ckpt, d.stepsum_part, 0);
   cudaError_t err = cudaMemsetAsync(d.ap, 0, sizeof(float) * d.V * kGainCols, stream);
   if (err != cudaSuccess) return err;
   err = cudaMemsetAsync(d.ap_last, 0, sizeof(float) * d.V * kGainCols, stream);
@@ -614,12 +704,10 @@ cudaError_t launch_forward(DeviceScenario& d, float threshold, float* ckpt, cuda
     r.hslot = d.hslot;
     r.nhalo = d.nhalo;
     void* args[] = {&a, &r};
-    return cudaLaunchCooperativeKernel((const void*)forward_ring_kernel, dim3(d.fwd_grid), dim3(kThreads), args,
-                                       sizeof(RingSmem), stream);
+    return launch_cooperative((const void*)forward_ring_kernel, d.fwd_grid, kThreads, args, sizeof(RingSmem), stream);
   }
   void* args[] = {&a};
-  return cudaLaunchCooperativeKernel((const void*)forward_stream_kernel, dim3(d.fwd_grid), dim3(kThreads), args,
-                                     sizeof(Smem), stream);
+  return launch_cooperative((const void*)forward_stream_kernel, d.fwd_grid, kThreads, args, sizeof(Smem), stream);
 }
 
 }  // namespace ct

@@ -56,4 +56,21 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int numb
   return s_ok != 0;
 }
 
+// Cooperative launch (all CTAs co-resident, required by grid_barrier) through cudaLaunchKernelExC with
+// the cooperative attribute, which stream capture records as a cooperative kernel node.
+inline cudaError_t launch_cooperative(const void* func, int grid, int block, void** args, size_t smem,
+                                      cudaStream_t stream) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, func, args);
+}
+
 }  // namespace ct

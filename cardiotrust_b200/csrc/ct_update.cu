@@ -20,10 +20,16 @@ __global__ void sgd_kernel(float* __restrict__ p, const float* __restrict__ g, i
   if (i < n) p[i] = p[i] - lr_over_bs * g[i];
 }
 
+// bias_dev, when set, holds {bias1, bias2} of this update (written by the host before a graph replay).
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m1,
-                            float* __restrict__ m2, int64_t n, float lr_over_bs, float bias1, float bias2) {
+                            float* __restrict__ m2, int64_t n, float lr_over_bs, float bias1, float bias2,
+                            const float* __restrict__ bias_dev) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (bias_dev) {
+    bias1 = bias_dev[0];
+    bias2 = bias_dev[1];
+  }
   const float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
   const float omb1 = 1.0f - beta1, omb2 = 1.0f - beta2;
   const float gi = g[i];
@@ -198,10 +204,22 @@ __global__ void step_metrics_kernel(const float* __restrict__ part, int grid, in
 
 // ---- metrics::calculate_batch (metrics.rs:204-219): means with ndarray's
 // eight-accumulator summation; thread q of each group runs accumulator q.
+// index_dev, when set, holds the slot (offset of o0/o1/o2) of this batch, read on the device.
 __global__ void batch_metrics_kernel(const float* __restrict__ a0, const float* __restrict__ a1,
                                      const float* __restrict__ a2, int64_t T, float* __restrict__ o0,
-                                     float* __restrict__ o1, float* __restrict__ o2) {
+                                     float* __restrict__ o1, float* __restrict__ o2, const int64_t* index_dev,
+                                     int64_t slots, int32_t* status) {
   __shared__ float p[3][8];
+  if (index_dev) {
+    const int64_t idx = *index_dev;
+    if (idx < 0 || idx >= slots) {
+      if (threadIdx.x == 0) atomicCAS(status, 0, (int32_t)CT_ERR_BATCH_INDEX);
+      return;
+    }
+    o0 += idx;
+    o1 += idx;
+    o2 += idx;
+  }
   const int which = threadIdx.x / 8, q = threadIdx.x % 8;
   const float* xs = which == 0 ? a0 : (which == 1 ? a1 : a2);
   const int64_t full = (T / 8) * 8;
@@ -258,14 +276,14 @@ cudaError_t launch_update(DeviceScenario& d, const UpdateScalars& s, cudaStream_
       sgd_kernel<<<blocks(ng, 256), 256, 0, stream>>>(d.gains, d.dG, ng, s.lr_over_bs);
     else
       adam_kernel<<<blocks(ng, 256), 256, 0, stream>>>(d.gains, d.dG, d.mG1, d.mG2, ng, s.lr_over_bs, s.bias1,
-                                                       s.bias2);
+                                                       s.bias2, s.bias_dev);
   }
   if (!s.freeze_delays) {
     if (s.optimizer == CT_OPT_SGD)
       sgd_kernel<<<blocks(nc, 256), 256, 0, stream>>>(d.coefs, d.dC, nc, s.lr_over_bs);
     else
       adam_kernel<<<blocks(nc, 256), 256, 0, stream>>>(d.coefs, d.dC, d.mC1, d.mC2, nc, s.lr_over_bs, s.bias1,
-                                                       s.bias2);
+                                                       s.bias2, s.bias_dev);
     roll_delays_kernel<<<blocks(nc, 256), 256, 0, stream>>>(d.coefs, d.delays, nc);
   }
   return cudaGetLastError();
@@ -296,7 +314,20 @@ cudaError_t launch_step_metrics(DeviceScenario& d, float reg_strength, cudaStrea
 
 cudaError_t launch_batch_metrics(DeviceScenario& d, int64_t index, cudaStream_t stream) {
   batch_metrics_kernel<<<1, 32, 0, stream>>>(d.loss_mse, d.loss_mr, d.loss, d.T, d.loss_mse_b + index,
-                                             d.loss_mr_b + index, d.loss_b + index);
+                                             d.loss_mr_b + index, d.loss_b + index, nullptr, 0, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_metrics_dev(DeviceScenario& d, const int64_t* index_dev, cudaStream_t stream) {
+  batch_metrics_kernel<<<1, 32, 0, stream>>>(d.loss_mse, d.loss_mr, d.loss, d.T, d.loss_mse_b, d.loss_mr_b, d.loss_b,
+                                             index_dev, d.NB, d.status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step_metrics_parts(DeviceScenario& d, const float* part, int parts, float reg_strength,
+                                      cudaStream_t stream) {
+  step_metrics_kernel<<<1, 1024, 0, stream>>>(part, parts, d.T, reg_strength, d.mreg_sum, d.loss_mse, d.loss_mr,
+                                              d.loss);
   return cudaGetLastError();
 }
 

@@ -611,3 +611,44 @@ def workload_spec(name: str, seed: int = 0) -> ScenarioSpec:
             shape=(64, 64, 48), mask="shell", num_steps=8000, num_sensors=256, patho_size=5, noise_fraction=0.01, seed=seed
         )
     raise ValueError(f"unknown workload {name!r}")
+
+
+def batch_workload_specs(count: int = 64, seed: int = 0) -> list:
+    """The batched workload: ``count`` scenarios of uneven size.
+
+    Each draws its voxel count log-uniformly from 500 to 30,000 (even
+    entries cuboids of random aspect, odd entries ellipsoidal shells scaled
+    from the 64x64x48 shell), 1 to 8 beats, 1,000 to 4,000 steps, 37 to 128
+    triaxial sensors, a random 3x3x3 pathological block and a random
+    control-pulse onset in the first tenth of the beat. Sizes are drawn from
+    ``seed``; every scenario has its own seed for the rest.
+    """
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        target = float(np.exp(rng.uniform(np.log(500.0), np.log(30000.0))))
+        beats = int(rng.integers(1, 9))
+        steps = int(rng.integers(1000, 4001))
+        sensors = int(rng.integers(37, 129))
+        onset = int(rng.integers(0, steps // 10))
+        if i % 2 == 0:
+            a, b = (float(x) for x in rng.uniform(0.8, 1.25, size=2))
+            edge = target ** (1.0 / 3.0)
+            nx = max(4, int(round(edge * a)))
+            ny = max(4, int(round(edge * b)))
+            nz = max(4, int(round(target / (nx * ny))))
+            spec = ScenarioSpec(shape=(nx, ny, nz), mask="cuboid")
+        else:
+            sc = (target / 47264.0) ** (1.0 / 3.0)
+            shape = (max(8, int(math.ceil(64 * sc))), max(8, int(math.ceil(64 * sc))), max(6, int(math.ceil(48 * sc))))
+            spec = ScenarioSpec(shape=shape, mask="shell", shell_semi_axes=(30.0 * sc, 25.0 * sc, 22.0 * sc),
+                                shell_thickness=max(2.0, 8.0 * sc))
+        spec.num_steps = steps
+        spec.num_beats = beats
+        spec.num_sensors = sensors
+        spec.patho_size = 3
+        spec.pulse_onset = onset
+        spec.noise_fraction = 0.01
+        spec.seed = seed * 1000 + i + 1
+        specs.append(spec)
+    return specs

@@ -173,6 +173,29 @@ int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, i
  * behaviour as ct_run_epoch. */
 int ct_run_epoch_plain(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order);
 
+/* ---- batched scenarios (no counterpart in the reference, which runs one scenario per OS
+ * thread, src/core/scheduler.rs:93).
+ * A batch runs one epoch of every member as one schedule: per beat index, one persistent
+ * forward launch over the tiles of every member that has that beat, the members' measurement
+ * products on parallel streams, one persistent adjoint launch (CT_GRAD_ADJOINT) or the members'
+ * reference derivations, then every member's update. The epoch is captured once as a CUDA
+ * graph and replayed (re-captured when a member's algorithm or adjoint ring changes).
+ * Members need batch_size 0 (one update per epoch, the reference default) and the same
+ * context; their beats run in index order. Results equal ct_run_epoch with beat_order
+ * 0..B-1 within the tolerances of the measurement products. The members stay usable on
+ * their own; a batch must be destroyed before its members. */
+typedef struct ct_batch ct_batch;
+int ct_batch_create(ct_ctx* ctx, ct_scn* const* scenarios, int64_t count, int grad_mode, int precision,
+                    ct_batch** out);
+int ct_batch_destroy(ct_batch* batch);
+/* One epoch of every member, enqueued on the context stream (asynchronous).
+ * batch_indices: in/out batch-wise metric cursor per member (as ct_run_epoch's batch_index). */
+int ct_batch_run_epoch(ct_batch* batch, int64_t* batch_indices);
+/* Waits for the batch and reports any device-side failure of a member. */
+int ct_batch_sync(ct_batch* batch);
+/* Kernel nodes in the captured epoch graph, and whether the graph is used (0: eager launches). */
+int ct_batch_info(ct_batch* batch, int64_t* graph_kernels, int* uses_graph);
+
 /* Forward of every beat with the current parameters (no noise); writes the predicted
  * measurements [B,T,M] and, if non-NULL, the states [T,S] of the last beat. Synchronous. */
 int ct_simulate(ct_scn* scn, float* measurements_out, float* states_out);
