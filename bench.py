@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--cpu-steps", type=int, default=200, help="steps of the bounded CPU sample")
     p.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "tf32"],
                    help="measurement products: FP32 CUDA cores, tcgen05 split TF32, tcgen05 TF32")
+    p.add_argument("--batch-scenarios", type=int, default=64,
+                   help="scenarios of the batched section (0 skips it)")
+    p.add_argument("--batch-epochs", type=int, default=3, help="timed epochs of the batched section")
     return p.parse_args()
 
 
@@ -207,6 +210,109 @@ def reference_arm(args):
 # ----------------------------------------------------------------------------------------- GPU
 
 
+def timed_epochs(stream, run, n, flush=None):
+    """Device time (ms) of `n` calls of `run`, each bracketed by CUDA events on `stream`."""
+    import torch
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    for k in range(n):
+        if flush is not None:
+            flush.random_(0, 255)
+        ev[k][0].record(stream)
+        run()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def forms_section(alg, eng, bi, prec, stream, flush, scn):
+    """The plain GPU form and the adjoint mode on the headline workload."""
+    V, T, B = scn.num_voxels, scn.num_steps, scn.num_beats
+    out = {}
+    bi = eng.run_epoch_plain(bi, sync=True)  # warm-up (allocates the plain form's buffers)
+    l0 = eng.kernel_launches()
+    ms = timed_epochs(stream, lambda: eng.run_epoch_plain(0, sync=False), 2, flush)
+    eng.sync()
+    launches = (eng.kernel_launches() - l0) // 2
+    bi += 2
+    out["plain"] = {"form": "plain GPU form: one launch per phase per step (reference gradients, FP32)",
+                    "scenario_epochs_per_s": 1000.0 / statistics.mean(ms), "ms_per_epoch": statistics.mean(ms),
+                    "voxel_steps_per_s": V * T * B * 1000.0 / statistics.mean(ms), "launches_per_epoch": int(launches)}
+    bi = eng.run_epoch(bi, grad_mode=alg.GradMode.Adjoint, precision=prec, sync=True)
+    eng.set_profiling(True)
+    ms = timed_epochs(stream, lambda: eng.run_epoch(0, grad_mode=alg.GradMode.Adjoint, precision=prec, sync=False),
+                      3, flush)
+    prof = eng.read_profile()
+    eng.set_profiling(False)
+    out["adjoint"] = {"form": "persistent kernels, adjoint gradients (checkpoints every 256 steps)",
+                      "scenario_epochs_per_s": 1000.0 / statistics.mean(ms), "ms_per_epoch": statistics.mean(ms),
+                      "voxel_steps_per_s": V * T * B * 1000.0 / statistics.mean(ms),
+                      "phase_ms": {k: v[0] / 3 for k, v in prof.items() if v[0] > 0}}
+    return out
+
+
+def batched_section(args, alg, sc, ctx, prec, stream, flush):
+    """64 scenarios of uneven size (batch_workload_specs): the batched adjoint epoch (one forward and
+    one adjoint launch per beat index over every member, replayed from a CUDA graph) against the plain
+    one-scenario GPU form run over every member in turn."""
+    import numpy as np
+
+    t0 = time.perf_counter()
+    specs = sc.batch_workload_specs(args.batch_scenarios, seed=0)
+    cfg = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False,
+                        ap_derivative=alg.APDerivative.Textbook)
+    engines, vtb, sizes = [], 0, []
+    slots = 2 + args.batch_epochs + 2
+    for sp in specs:
+        scn = sc.build(sp)
+        truth = alg.EpochEngine.from_scenario(ctx, scn, truth=True)
+        y = truth.simulate()
+        truth.close()
+        rng = np.random.default_rng(sp.seed + 7919)
+        sigma = sp.noise_fraction * float(np.sqrt(np.mean(y.astype(np.float64) ** 2)))
+        scn.measurements = (y + rng.normal(0.0, sigma, size=y.shape)).astype(np.float32)
+        engines.append(alg.EpochEngine.from_scenario(ctx, scn, num_batch_slots=slots, algorithm=cfg))
+        vtb += scn.num_voxels * scn.num_steps * scn.num_beats
+        sizes.append(scn.num_voxels)
+        del scn
+    build_s = time.perf_counter() - t0
+    usable_prec = prec if all(e.dims["S"] % 4 == 0 for e in engines) else alg.Precision.Fp32
+    batch = alg.EpochBatch(ctx, engines, grad_mode=alg.GradMode.Adjoint, precision=usable_prec)
+    batch.run_epoch(sync=True)  # warm-up: captures the epoch graph
+    ms = timed_epochs(stream, lambda: batch.run_epoch(sync=False), args.batch_epochs, flush)
+    batch.sync()
+    info = batch.info()
+    chosen_ms = statistics.mean(ms)
+    n = len(engines)
+    # plain one-scenario form over every member, one epoch each (after one warm-up epoch of the smallest)
+    small = int(np.argmin(sizes))
+    engines[small].run_epoch_plain(int(batch.batch_indices[small]), sync=True)
+    plain_ms = 0.0
+    for k, e in enumerate(engines):
+        plain_ms += timed_epochs(stream, lambda: e.run_epoch_plain(0 if k != small else 1, sync=False), 1)[0]
+    batch.close()
+    for e in engines:
+        e.close()
+    chosen = n * 1000.0 / chosen_ms
+    plain = n * 1000.0 / plain_ms
+    return {
+        "workload": f"{n} scenarios: voxels log-uniform 500..30000 (cuboids and shells), 1-8 beats, 1000-4000 "
+                    "steps, 37-128 triaxial sensors, random 3^3 pathological block and pulse onset, Adam lr 1e-3, "
+                    "gains+coefficients",
+        "scenarios": n, "voxels_total": int(sum(sizes)), "voxel_steps_per_epoch": int(vtb),
+        "build_s": build_s,
+        "chosen": {"form": "batched: one persistent forward and one persistent adjoint launch per beat index over "
+                           "every member's tiles, epoch replayed from a CUDA graph; adjoint gradients, checkpoints "
+                           "every 64 steps", "precision": ["fp32", "tf32x3", "tf32"][int(usable_prec)],
+                   "scenario_epochs_per_s": chosen, "voxel_steps_per_s": vtb * 1000.0 / chosen_ms,
+                   "ms_per_epoch": chosen_ms, "graph_kernels": info["graph_kernels"], "uses_graph": info["uses_graph"]},
+        "plain": {"form": "plain GPU form, one scenario at a time, one launch per phase per step (reference "
+                          "gradients, FP32)", "scenario_epochs_per_s": plain,
+                  "voxel_steps_per_s": vtb * 1000.0 / plain_ms, "ms_per_epoch_all": plain_ms},
+        "chosen_vs_plain": chosen / plain,
+    }
+
+
 def gpu_arm(args):
     import numpy as np
     import torch
@@ -332,6 +438,13 @@ def gpu_arm(args):
                 "frac": achieved / hbm_peak, "peak_source": peak_src, "traffic": None,
                 "algorithmic_bytes_per_launch": algo_bytes[rl_kernel], "launch_ms": per_launch_ms}
 
+    # ---- plain GPU form and adjoint mode on the same workload; the batched workload
+    forms = forms_section(alg, eng, bi, prec, stream, flush, scn)
+    batched = None
+    if args.batch_scenarios > 0 and world == 1:
+        eng.close()
+        batched = batched_section(args, alg, sc, ctx, prec, stream, flush)
+
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
     if rank == 0 and world == 1:
@@ -376,6 +489,9 @@ def gpu_arm(args):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "clocks": clock,
+            "forms": forms,
+            "chosen_vs_plain": value / forms["plain"]["scenario_epochs_per_s"],
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     eng.close()

@@ -15,8 +15,8 @@
 //
 // Schedule (one cooperative launch per beat, or per beat of a batch of
 // scenarios: every tile names its scenario):
-//   * Checkpoints. The forward stores the all-pass state every kCkptSteps
-//     steps. Segments are visited from the last to the first; a CTA first
+//   * Checkpoints. The forward stores the all-pass state every K steps
+//     (K a power of two, 256 by default). Segments are visited from the last to the first; a CTA first
 //     recomputes, from the checkpoint and the stored states, ap[t] and
 //     q[t] = in_t - ap[t-1] of its own tiles for the segment (the forward's
 //     fmaf, so bit-identical), then steps the segment backwards.
@@ -27,7 +27,7 @@
 //     at a time between grid barriers, as in the forward. A voxel's 78 inbox
 //     cells are contiguous and summed in column order, so results are
 //     deterministic (no atomics).
-//   * Pipeline. Thread e owns tile columns e, e+256, ... A step's inbox row
+//   * Pipeline. Thread e owns tile columns e, e+512, ... A step's inbox row
 //     and recomputed ap/q rows (contiguous per tile; plane pitch padded to 16
 //     bytes) arrive by TMA bulk copies into a ring of kStages shared-memory
 //     stages, issued kStages steps ahead by one thread and completed on an
@@ -44,22 +44,30 @@ namespace ct {
 namespace {
 
 constexpr int kTileVoxels = kFwdTileVoxels;
-constexpr int kTileStates = 3 * kTileVoxels;
 constexpr int kTileCols = kTileVoxels * kGainCols;
-constexpr int kAdjThreads = 256;
-constexpr int kCols = (kTileCols + kAdjThreads - 1) / kAdjThreads;  // 10 columns per thread
+constexpr int kTileItems = kTileVoxels * kOffsets;
+constexpr int kAdjThreads = 512;
+constexpr int kGroup = 16;                 // threads per voxel (a half warp)
+constexpr int kCols = 5;                   // columns per thread: k = lane + 16 i, k < 78
+constexpr int kWarps = kAdjThreads / 32;
 constexpr int kStages = 4;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every mbarrier wait
+static_assert(kTileVoxels * kGroup == kAdjThreads, "one voxel group per 16 threads");
+static_assert(kCols * kGroup >= kGainCols, "columns per voxel");
 
 struct AdjSmem {
-  float g3[3][kTileCols];              // gains of the voxel's rows a = 0, 1, 2 at each column
-  float stage[kStages][3][kTileCols];  // [stage][inbox | ap | q][column]
-  float lx[kTileStates];
-  uint64_t bar[kStages];
-  uint32_t phase;                      // bit s: parity of the next completion of stage s
-  uint32_t pending;                    // bit s: a copy into stage s is in flight
+  float g[kTileVoxels * 3 * kGainCols];  // the tile's gain rows, [voxel][row a][column k] as in HBM
+  float stage[kStages][3][kTileCols];    // [stage][inbox | ap | q][voxel * 78 + column]
+  float xm[kStages][kTileVoxels][8];     // [stage][voxel][x0 x1 x2 mr0 mr1 mr2 - -]
+  float coef[kTileItems];                // per (voxel, offset) of the tile
+  int32_t del[kTileItems];
+  int32_t nbr[kTileItems];
+  float lam[kTileCols];                  // adjoint state carried between blocks (tiles that are not resident)
+  uint64_t full[kStages];                // the stage's rows have landed
+  uint64_t empty[kStages];               // every warp is done with the stage
+  uint64_t meta_bar;
   int abort;
-  AdjScn sp;                           // scenario of the current tile
+  AdjScn sp;                             // scenario of the current tile
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -69,6 +77,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
@@ -99,6 +110,14 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 __device__ __forceinline__ void red_add(float* p, float v) {
   asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }
@@ -126,33 +145,38 @@ __device__ __forceinline__ void load_scn(AdjSmem& sm, const AdjLaunch& L, int sc
   __syncthreads();
 }
 
-// ap[t] and q[t] = in_t - ap[t-1] of the tile's columns for steps [t_lo, t_hi) (own columns only).
+// The thread's voxel in the tile and its column i (valid when < 78).
+__device__ __forceinline__ int my_voxel() { return threadIdx.x / kGroup; }
+__device__ __forceinline__ int my_col(int i) { return (int)(threadIdx.x % kGroup) + kGroup * i; }
+
+// ap[t] and q[t] = in_t - ap[t-1] of the thread's columns for steps [t_lo, t_hi).
 __device__ __forceinline__ void recompute_segment(const AdjScn& p, int v0, int nv, int seg, int t_lo, int t_hi) {
   const size_t plane = (size_t)p.V * kGainCols;  // checkpoint planes are unpadded
   const size_t pitch = (size_t)p.pitch;
+  const int vl = my_voxel();
   float a[kCols], inp[kCols], c[kCols];
   const float* xs[kCols];
   int d[kCols];
 #pragma unroll
   for (int i = 0; i < kCols; ++i) {
-    const int e = threadIdx.x + i * kAdjThreads;
+    const int k = my_col(i);
     a[i] = inp[i] = c[i] = 0.0f;
     d[i] = 1 << 30;  // absent: every input reads as zero
     xs[i] = p.X;
-    if (e < nv * kGainCols) {
-      const int vl = e / kGainCols, k = e - vl * kGainCols, n = k / 3, b = k - 3 * n;
+    if (vl < nv && k < kGainCols) {
+      const int n = k / 3, b = k - 3 * n;
       const int v = v0 + vl;
       const int32_t nb = p.nbr[(size_t)v * kOffsets + n];
       if (nb >= 0) {
         d[i] = p.delays[(size_t)v * kOffsets + n];
         c[i] = p.coefs[(size_t)v * kOffsets + n];
         xs[i] = p.X + 3 * nb + b;
-        a[i] = p.ckpt[(size_t)seg * plane + (size_t)v0 * kGainCols + e];
+        a[i] = p.ckpt[(size_t)seg * plane + (size_t)v * kGainCols + k];
         inp[i] = (t_lo - d[i] - 1 >= 0) ? xs[i][(size_t)(t_lo - d[i] - 1) * p.S] : 0.0f;
       }
     }
   }
-  constexpr int kU = 4;
+  constexpr int kU = 2;
   for (int t0 = t_lo; t0 < t_hi; t0 += kU) {
     float in[kU][kCols];
 #pragma unroll
@@ -166,17 +190,17 @@ __device__ __forceinline__ void recompute_segment(const AdjScn& p, int v0, int n
     for (int u = 0; u < kU; ++u) {
       const int t = t0 + u;
       if (t < t_hi) {
-        float* sa = p.seg_ap + (size_t)(t - t_lo) * pitch + (size_t)v0 * kGainCols;
-        float* sq = p.seg_q + (size_t)(t - t_lo) * pitch + (size_t)v0 * kGainCols;
+        float* sa = p.seg_ap + (size_t)(t - t_lo) * pitch + (size_t)(v0 + vl) * kGainCols;
+        float* sq = p.seg_q + (size_t)(t - t_lo) * pitch + (size_t)(v0 + vl) * kGainCols;
 #pragma unroll
         for (int i = 0; i < kCols; ++i) {
-          const int e = threadIdx.x + i * kAdjThreads;
+          const int k = my_col(i);
           const float q = in[u][i] - a[i];
           a[i] = fmaf(c[i], q, inp[i]);
           inp[i] = in[u][i];
-          if (e < nv * kGainCols) {
-            sa[e] = a[i];
-            sq[e] = q;
+          if (vl < nv && k < kGainCols) {
+            sa[k] = a[i];
+            sq[k] = q;
           }
         }
       }
@@ -184,53 +208,67 @@ __device__ __forceinline__ void recompute_segment(const AdjScn& p, int v0, int n
   }
 }
 
-// Per-column registers of the tile a thread works on.
+// Per-column registers of the tile a thread works on, and the thread's stage-barrier phases.
 struct Cols {
   float c[kCols], lprev[kCols], dg[kCols][3], dc[kCols];
   int d[kCols], jw[kCols];  // delay; inbox cell neighbour * 78 + column, -1 if unconnected
+  uint32_t full_ph;         // bit s: parity of the next completion of full[s]
+  uint32_t empty_ph;        // thread 0: parity of the next completion of empty[s]
+  uint32_t empty_wait;      // thread 0: bit s: a use of stage s has not been waited empty yet
+  uint32_t inflight;        // thread 0: bit s: copies into stage s issued and not yet waited full
+  uint32_t meta_ph;
 };
 
-__device__ __forceinline__ void load_cols(Cols& cs, AdjSmem& sm, const AdjScn& p, int v0, int nv, bool state) {
+// Per-tile tables into shared memory by bulk copies (gains, coefficients, delays, neighbours and,
+// with `state`, the adjoint state of the previous block), then each thread's column registers.
+// Called by all threads after a CTA barrier.
+__device__ __forceinline__ bool load_cols(Cols& cs, AdjSmem& sm, const AdjScn& p, int v0, int nv, bool state,
+                                          int32_t* status) {
+  if (threadIdx.x == 0) {
+    const uint32_t gb = (uint32_t)((nv * 3 * kGainCols * 4 + 15) & ~15);
+    const uint32_t ib = (uint32_t)((nv * kOffsets * 4 + 15) & ~15);
+    const uint32_t lb = (uint32_t)((nv * kGainCols * 4 + 15) & ~15);
+    asm volatile("fence.proxy.async;" ::: "memory");
+    mbar_expect_tx(&sm.meta_bar, gb + 3 * ib + (state ? lb : 0));
+    bulk_load(sm.g, p.gains + (size_t)3 * v0 * kGainCols, gb, &sm.meta_bar);
+    bulk_load(sm.coef, p.coefs + (size_t)v0 * kOffsets, ib, &sm.meta_bar);
+    bulk_load(sm.del, p.delays + (size_t)v0 * kOffsets, ib, &sm.meta_bar);
+    bulk_load(sm.nbr, p.nbr + (size_t)v0 * kOffsets, ib, &sm.meta_bar);
+    if (state) bulk_load(sm.lam, p.lam_state + (size_t)v0 * kGainCols, lb, &sm.meta_bar);
+  }
+  const bool ok = mbar_wait(&sm.meta_bar, cs.meta_ph, status);
+  cs.meta_ph ^= 1u;
+  const int vl = my_voxel();
 #pragma unroll
   for (int i = 0; i < kCols; ++i) {
-    const int e = threadIdx.x + i * kAdjThreads;
+    const int k = my_col(i);
     cs.c[i] = 0.0f;
     cs.d[i] = 1 << 30;
     cs.jw[i] = -1;
     cs.lprev[i] = 0.0f;
-    float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
-    if (e < nv * kGainCols) {
-      const int vl = e / kGainCols, k = e - vl * kGainCols, n = k / 3;
-      const int v = v0 + vl;
-      const int32_t nb = p.nbr[(size_t)v * kOffsets + n];
+    if (ok && vl < nv && k < kGainCols) {
+      const int it = vl * kOffsets + k / 3;
+      const int32_t nb = sm.nbr[it];
       if (nb >= 0) {
-        cs.c[i] = p.coefs[(size_t)v * kOffsets + n];
-        cs.d[i] = p.delays[(size_t)v * kOffsets + n];
+        cs.c[i] = sm.coef[it];
+        cs.d[i] = sm.del[it];
         cs.jw[i] = nb * kGainCols + k;
-        const float* g = p.gains + (size_t)3 * v * kGainCols + k;
-        g0 = g[0];
-        g1 = g[kGainCols];
-        g2 = g[2 * kGainCols];
       }
-      if (state) cs.lprev[i] = p.lam_state[(size_t)v0 * kGainCols + e];
-    }
-    if (e < kTileCols) {
-      sm.g3[0][e] = g0;
-      sm.g3[1][e] = g1;
-      sm.g3[2][e] = g2;
+      if (state) cs.lprev[i] = sm.lam[vl * kGainCols + k];
     }
     cs.dg[i][0] = cs.dg[i][1] = cs.dg[i][2] = 0.0f;
     cs.dc[i] = 0.0f;
   }
+  return ok;
 }
 
 // Add the columns' gradient sums to dG / dCk (and keep their adjoint state for the next block).
 __device__ __forceinline__ void flush_cols(Cols& cs, const AdjScn& p, int v0, int nv, bool keep_state) {
+  const int vl = my_voxel();
 #pragma unroll
   for (int i = 0; i < kCols; ++i) {
-    const int e = threadIdx.x + i * kAdjThreads;
-    if (e < nv * kGainCols) {
-      const int vl = e / kGainCols, k = e - vl * kGainCols;
+    const int k = my_col(i);
+    if (vl < nv && k < kGainCols) {
       const int v = v0 + vl;
       // one owner per element, adds ordered by the grid barriers: a deterministic sum
       if (!p.freeze_gains) {
@@ -239,121 +277,143 @@ __device__ __forceinline__ void flush_cols(Cols& cs, const AdjScn& p, int v0, in
         red_add(g + kGainCols, cs.dg[i][1]);
         red_add(g + 2 * kGainCols, cs.dg[i][2]);
       }
-      red_add(p.dCk + (size_t)v0 * kGainCols + e, cs.dc[i]);
-      if (keep_state) p.lam_state[(size_t)v0 * kGainCols + e] = cs.lprev[i];
+      red_add(p.dCk + (size_t)v * kGainCols + k, cs.dc[i]);
+      if (keep_state) p.lam_state[(size_t)v * kGainCols + k] = cs.lprev[i];
     }
     cs.dg[i][0] = cs.dg[i][1] = cs.dg[i][2] = 0.0f;
     cs.dc[i] = 0.0f;
   }
 }
 
-// Thread 0: bulk copies of step t's inbox, ap and q rows of the tile into stage `st`.
-__device__ __forceinline__ void issue_stage(AdjSmem& sm, const AdjScn& p, int st, int v0, int nv, int t, int t_lo) {
+// Thread 0: bulk copies of step t's inbox, ap and q rows of the tile into stage `st`, once every
+// warp has released the stage's previous use.
+__device__ __forceinline__ bool issue_stage(Cols& cs, AdjSmem& sm, const AdjScn& p, int st, int v0, int nv, int t,
+                                           int t_lo, int32_t* status) {
+  if (cs.empty_wait & (1u << st)) {
+    if (!mbar_wait(&sm.empty[st], (cs.empty_ph >> st) & 1u, status)) return false;
+    cs.empty_ph ^= 1u << st;
+    cs.empty_wait &= ~(1u << st);
+  }
   const size_t pitch = (size_t)p.pitch;
   const uint32_t bytes = (uint32_t)(((nv * kGainCols * 4) + 15) & ~15);  // stays inside the padded row
-  mbar_expect_tx(&sm.bar[st], 3 * bytes);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_expect_tx(&sm.full[st], 3 * bytes);
   bulk_load(sm.stage[st][0], p.inbox + (size_t)(t & (p.ring - 1)) * pitch + (size_t)v0 * kGainCols, bytes,
-            &sm.bar[st]);
-  bulk_load(sm.stage[st][1], p.seg_ap + (size_t)(t - t_lo) * pitch + (size_t)v0 * kGainCols, bytes, &sm.bar[st]);
-  bulk_load(sm.stage[st][2], p.seg_q + (size_t)(t - t_lo) * pitch + (size_t)v0 * kGainCols, bytes, &sm.bar[st]);
-  sm.pending |= 1u << st;
+            &sm.full[st]);
+  bulk_load(sm.stage[st][1], p.seg_ap + (size_t)(t - t_lo) * pitch + (size_t)v0 * kGainCols, bytes, &sm.full[st]);
+  bulk_load(sm.stage[st][2], p.seg_q + (size_t)(t - t_lo) * pitch + (size_t)v0 * kGainCols, bytes, &sm.full[st]);
+  cs.empty_wait |= 1u << st;
+  cs.inflight |= 1u << st;
+  return true;
 }
 
-// After a timed-out wait: let every copy still in flight land (bounded) before the CTA leaves.
-__device__ __forceinline__ void drain_stages(AdjSmem& sm, int32_t* status) {
-  if (threadIdx.x == 0)
-    for (int st = 0; st < kStages; ++st)
-      if (sm.pending & (1u << st)) mbar_wait(&sm.bar[st], (sm.phase >> st) & 1u, status);
+// Threads 0-5 of each voxel group: the voxel's states and mapped residuals of step t into stage
+// `st` (one cp.async group per stage and thread, committed even when empty).
+__device__ __forceinline__ void issue_xm(AdjSmem& sm, const AdjScn& p, int st, int v0, int nv, int t, bool real) {
+  const int vl = my_voxel(), q = threadIdx.x % kGroup;
+  if (real && vl < nv && q < 6) {
+    const size_t off = (size_t)t * p.S + 3 * (v0 + vl) + (q % 3);
+    cp_async4(&sm.xm[st][vl][q], (q < 3 ? p.X : p.MR) + off);
+  }
+  cp_async_commit();
 }
 
 // Steps ta down to t_end (inclusive) of one tile; t_lo is the segment's first step (row 0 of seg_ap/seg_q).
+// Warps run decoupled: a step's rows arrive on full[st], each warp releases them on empty[st].
 // Returns false if a wait timed out (the CTA must leave).
 __device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem& sm, const AdjScn& p, int v0, int nv, int ta,
                                                int t_end, int t_lo, int32_t* status) {
   const size_t pitch = (size_t)p.pitch;
   const int rmask = p.ring - 1;
-  const int S = p.S;
-  const bool lxt = (int)threadIdx.x < 3 * nv;  // implies < kTileStates
-  const int vlx = threadIdx.x / 3;
-  // every generic write this CTA's copies read (recomputed rows, inbox cells of earlier blocks,
-  // made visible by the grid barrier) is ordered before the async-proxy reads
+  const int vl = my_voxel();
+  const int lane = threadIdx.x & 31;
+  const bool live = vl < nv;
+  // thread 0 orders every generic write these copies read (recomputed rows, inbox cells of earlier
+  // blocks, made visible by the grid barrier) before the async-proxy reads, in issue_stage
   if (threadIdx.x == 0) {
     asm volatile("fence.proxy.async;" ::: "memory");
-    for (int s = 0; s < kStages && ta - s >= t_end; ++s) issue_stage(sm, p, s, v0, nv, ta - s, t_lo);
+    for (int s = 0; s < kStages && ta - s >= t_end; ++s)
+      if (!issue_stage(cs, sm, p, s, v0, nv, ta - s, t_lo, status)) sm.abort = 1;
   }
-  float mr_n = 0.0f, x0_n = 0.0f, x1_n = 0.0f, x2_n = 0.0f;
-  if (lxt) {
-    const float* x = p.X + (size_t)ta * S + 3 * (v0 + vlx);
-    mr_n = p.MR[(size_t)ta * S + 3 * v0 + threadIdx.x];
-    x0_n = x[0];
-    x1_n = x[1];
-    x2_n = x[2];
-  }
+  for (int s = 0; s < kStages; ++s) issue_xm(sm, p, s, v0, nv, ta - s, ta - s >= t_end);
   for (int t = ta; t >= t_end; --t) {
     const int st = (ta - t) % kStages;
-    const float mr = mr_n, x0 = x0_n, x1 = x1_n, x2 = x2_n;
-    if (lxt && t - 1 >= t_end) {
-      const float* x = p.X + (size_t)(t - 1) * S + 3 * (v0 + vlx);
-      mr_n = p.MR[(size_t)(t - 1) * S + 3 * v0 + threadIdx.x];
-      x0_n = x[0];
-      x1_n = x[1];
-      x2_n = x[2];
+    if (*(volatile int*)&sm.abort) return false;
+    if (!mbar_wait(&sm.full[st], (cs.full_ph >> st) & 1u, status)) {
+      sm.abort = 1;
+      return false;
     }
-    const uint32_t par = (sm.phase >> st) & 1u;
-    if (!mbar_wait(&sm.bar[st], par, status)) sm.abort = 1;
-    __syncthreads();  // (A) every thread past the wait; abort visible
-    if (sm.abort) return false;
-    // lx[t] of the tile's states: instantaneous terms + inbox, summed in column order
-    if (threadIdx.x < kTileStates) {
-      const int b = threadIdx.x - 3 * vlx;
-      float lx = 0.0f;
-      if (lxt) {
-        const float sum = fabsf(x0) + fabsf(x1) + fabsf(x2);
-        const float f = sum > p.threshold ? sum - p.threshold : 0.0f;
-        const float xb = b == 0 ? x0 : (b == 1 ? x1 : x2);
-        const float mreg = f > 0.0f ? f * copysignf(1.0f, xb) : 0.0f;
-        const float* pl = sm.stage[st][0] + vlx * kGainCols + b;
-        float acc = 0.0f;
-#pragma unroll
-        for (int n = 0; n < kOffsets; ++n) acc = acc + pl[3 * n];
-        lx = p.mse_scaling * mr + p.reg_scaling * mreg + acc;
-      }
-      sm.lx[threadIdx.x] = lx;
-    }
-    __syncthreads();  // (B)
-    if (threadIdx.x == 0) sm.phase ^= 1u << st;
-    // the tile's columns: lap[t], gradient sums, inbox cell of the neighbour at step t - d
+    cs.full_ph ^= 1u << st;
+    cs.inflight &= ~(1u << st);
+    cp_async_wait<kStages - 1>();  // this thread's copies of step t
+    __syncwarp();                  // the voxel group's copies of step t
+    // lx[t] of the voxel: instantaneous terms + its 78 inbox cells (partial sums per component,
+    // reduced over the 16-thread group in a fixed order)
+    float pb[3] = {0.0f, 0.0f, 0.0f};
+    const float* in_row = sm.stage[st][0] + vl * kGainCols;
 #pragma unroll
     for (int i = 0; i < kCols; ++i) {
-      const int e = threadIdx.x + i * kAdjThreads;
+      const int k = my_col(i);
+      if (k < kGainCols) {
+        const float v = in_row[k];
+        const int b = k % 3;
+        pb[0] = pb[0] + (b == 0 ? v : 0.0f);
+        pb[1] = pb[1] + (b == 1 ? v : 0.0f);
+        pb[2] = pb[2] + (b == 2 ? v : 0.0f);
+      }
+    }
+#pragma unroll
+    for (int off = kGroup / 2; off > 0; off >>= 1)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) pb[b] = pb[b] + __shfl_xor_sync(0xffffffffu, pb[b], off);
+    float lx[3] = {0.0f, 0.0f, 0.0f};
+    if (live) {
+      const float* xm = sm.xm[st][vl];
+      const float x0 = xm[0], x1 = xm[1], x2 = xm[2];
+      const float sum = fabsf(x0) + fabsf(x1) + fabsf(x2);
+      const float f = sum > p.threshold ? sum - p.threshold : 0.0f;
+      const float xs[3] = {x0, x1, x2};
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const float mreg = f > 0.0f ? f * copysignf(1.0f, xs[b]) : 0.0f;
+        lx[b] = p.mse_scaling * xm[3 + b] + p.reg_scaling * mreg + pb[b];
+      }
+    }
+    // the thread's columns: lap[t], gradient sums, inbox cell of the neighbour at step t - d
+    const float* g = sm.g + vl * (3 * kGainCols);
+#pragma unroll
+    for (int i = 0; i < kCols; ++i) {
+      const int k = my_col(i);
       if (cs.jw[i] >= 0) {
-        const int vl = e / kGainCols;
-        const float l0 = sm.lx[3 * vl], l1 = sm.lx[3 * vl + 1], l2 = sm.lx[3 * vl + 2];
-        const float G = sm.g3[0][e] * l0 + sm.g3[1][e] * l1 + sm.g3[2][e] * l2;
+        const float G = g[k] * lx[0] + g[kGainCols + k] * lx[1] + g[2 * kGainCols + k] * lx[2];
         const float lap = G - cs.c[i] * cs.lprev[i];
-        const float ap_t = sm.stage[st][1][e];
-        cs.dg[i][0] = cs.dg[i][0] + l0 * ap_t;
-        cs.dg[i][1] = cs.dg[i][1] + l1 * ap_t;
-        cs.dg[i][2] = cs.dg[i][2] + l2 * ap_t;
-        cs.dc[i] = cs.dc[i] + lap * sm.stage[st][2][e];
+        const float ap_t = sm.stage[st][1][vl * kGainCols + k];
+        cs.dg[i][0] = cs.dg[i][0] + lx[0] * ap_t;
+        cs.dg[i][1] = cs.dg[i][1] + lx[1] * ap_t;
+        cs.dg[i][2] = cs.dg[i][2] + lx[2] * ap_t;
+        cs.dc[i] = cs.dc[i] + lap * sm.stage[st][2][vl * kGainCols + k];
         const int ts = t - cs.d[i];
         if (ts >= 0) p.inbox[(size_t)(ts & rmask) * pitch + cs.jw[i]] = cs.c[i] * lap + cs.lprev[i];
         cs.lprev[i] = lap;
       }
     }
-    __syncthreads();  // (C) stage st and lx free again
-    if (threadIdx.x == 0) {
-      sm.pending &= ~(1u << st);
-      if (t - kStages >= t_end) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue_stage(sm, p, st, v0, nv, t - kStages, t_lo);
-      }
-    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.empty[st]);
+    issue_xm(sm, p, st, v0, nv, t - kStages, t - kStages >= t_end);
+    if (threadIdx.x == 0 && t - kStages >= t_end)
+      if (!issue_stage(cs, sm, p, st, v0, nv, t - kStages, t_lo, status)) sm.abort = 1;
   }
   return true;
 }
 
-__global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjLaunch L) {
+// After a timed-out wait: let every bulk copy still in flight land (bounded) before the CTA leaves.
+__device__ __forceinline__ void drain_stages(Cols& cs, AdjSmem& sm, int32_t* status) {
+  if (threadIdx.x == 0)
+    for (int st = 0; st < kStages; ++st)
+      if (cs.inflight & (1u << st)) mbar_wait(&sm.full[st], (cs.full_ph >> st) & 1u, status);
+}
+
+__global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjLaunch L) {  // <= 128 registers
   extern __shared__ __align__(16) unsigned char smem_raw[];
   AdjSmem& sm = *reinterpret_cast<AdjSmem*>(smem_raw);
   const int ntiles = L.ntiles;
@@ -374,23 +434,25 @@ __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjLaunch L) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(L.status, 0, (int32_t)CT_ERR_NOT_SUPPORTED);
     return;
   }
-
   if (threadIdx.x == 0) {
-    for (int st = 0; st < kStages; ++st) mbar_init(&sm.bar[st], 1);
-    sm.phase = 0;
-    sm.pending = 0;
+    for (int st = 0; st < kStages; ++st) {
+      mbar_init(&sm.full[st], 1);
+      mbar_init(&sm.empty[st], kWarps);
+    }
+    mbar_init(&sm.meta_bar, 1);
     sm.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
   Cols cs;
+  cs.full_ph = cs.empty_ph = cs.empty_wait = cs.inflight = cs.meta_ph = 0;
   int cur_scn = -1, v0 = 0, nv = 0;
   if (resident && (int)blockIdx.x < ntiles) {
     tile_of(L, blockIdx.x, &cur_scn, &v0);
     load_scn(sm, L, cur_scn);
     nv = min(kTileVoxels, sm.sp.V - v0);
-    load_cols(cs, sm, sm.sp, v0, nv, false);
+    if (!load_cols(cs, sm, sm.sp, v0, nv, false, L.status)) return;
   }
 
   unsigned int barrier_number = 0;
@@ -423,13 +485,10 @@ __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjLaunch L) {
         }
         const int ta = min(tb, sm.sp.T - 1);
         if (ta < t_end) continue;  // this tile's scenario ends before the block (uniform per CTA)
-        if (!resident) {
-          __syncthreads();
-          load_cols(cs, sm, sm.sp, v0, nv, true);
-        }
-        __syncthreads();
+        __syncthreads();  // recomputed rows (and the previous tile's tables) done with by every thread
+        if (!resident && !load_cols(cs, sm, sm.sp, v0, nv, true, L.status)) return;
         if (!backward_block(cs, sm, sm.sp, v0, nv, ta, t_end, t_lo, L.status)) {
-          drain_stages(sm, L.status);
+          drain_stages(cs, sm, L.status);
           return;
         }
         if (!resident) flush_cols(cs, sm.sp, v0, nv, true);
@@ -471,6 +530,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjLaunch L) {
     for (int e = threadIdx.x; e < nv * kGainCols; e += blockDim.x) p.dCk[(size_t)v0 * kGainCols + e] = 0.0f;
   }
 }
+
 
 bool configure(int device) {
   static bool done[128] = {};
@@ -553,7 +613,7 @@ cudaError_t launch_adjoint(DeviceScenario& d, const AdjointScalars& s, cudaStrea
   l.tiles = nullptr;
   l.ntiles = (int)((d.V + kTileVoxels - 1) / kTileVoxels);
   l.Tmax = (int)d.T;
-  l.ckpt_steps = kCkptSteps;
+  l.ckpt_steps = d.ckpt_k;
   l.status = d.status;
   l.barrier = d.barrier;
   return launch_adjoint_tiles(l, d.adj_grid, stream);

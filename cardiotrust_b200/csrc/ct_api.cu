@@ -208,11 +208,18 @@ void refresh_delay_bound(ct_scn* s) {
   s->updates_at_read = -1;
 }
 
-// Adjoint-mode buffers, allocated on first use; the ring grows with the delay bound.
-int prepare_adjoint(ct_scn* s) {
+// Adjoint-mode buffers, allocated on first use (or when the checkpoint interval k changes); the
+// inbox ring grows with the delay bound.
+int prepare_adjoint(ct_scn* s, int k = ct::kCkptSteps) {
   DeviceScenario& d = s->d;
   cudaStream_t st = s->ctx->stream;
   const int64_t V = d.V, plane = d.V * kGainCols;
+  if (d.rev && d.ckpt_k != k) {  // re-made below with the new interval
+    CT_CUDA(cudaStreamSynchronize(st), "adjoint re-layout");
+    for (void* p : {(void*)d.rev, (void*)d.ckpt, (void*)d.seg_ap, (void*)d.seg_q}) release(s, p);
+    d.rev = nullptr;
+    d.ckpt = d.seg_ap = d.seg_q = nullptr;
+  }
   if (!d.rev) {
     std::vector<int32_t> rev((size_t)(V * kOffsets), -1);
     for (int64_t v = 0; v < V; ++v)
@@ -225,18 +232,19 @@ int prepare_adjoint(ct_scn* s) {
                       "adjoint mode: two voxels reach the same neighbour along one offset (not a lattice)");
         slot = (int32_t)v;
       }
-    const int64_t nseg = (d.T + ct::kCkptSteps - 1) / ct::kCkptSteps;
-    const int64_t seg_steps = std::min<int64_t>(d.T, ct::kCkptSteps);
+    const int64_t nseg = (d.T + k - 1) / k;
+    const int64_t seg_steps = std::min<int64_t>(d.T, k);
     d.adj_pitch = (int)(((plane + 3) / 4) * 4);
+    d.ckpt_k = k;
     int rc = alloc(s, &d.rev, V * kOffsets);
     if (!rc) rc = alloc(s, &d.ckpt, nseg * plane);
     if (!rc) rc = alloc(s, &d.seg_ap, seg_steps * d.adj_pitch);
     if (!rc) rc = alloc(s, &d.seg_q, seg_steps * d.adj_pitch);
-    if (!rc) rc = alloc(s, &d.dCk, plane);
+    if (!rc && !d.dCk) rc = alloc(s, &d.dCk, plane);
     if (rc) {
-      for (void* p : {(void*)d.rev, (void*)d.ckpt, (void*)d.seg_ap, (void*)d.seg_q, (void*)d.dCk}) release(s, p);
+      for (void* p : {(void*)d.rev, (void*)d.ckpt, (void*)d.seg_ap, (void*)d.seg_q}) release(s, p);
       d.rev = nullptr;
-      d.ckpt = d.seg_ap = d.seg_q = d.dCk = nullptr;
+      d.ckpt = d.seg_ap = d.seg_q = nullptr;
       return rc;
     }
     CT_CUDA(cudaMemcpyAsync(d.rev, rev.data(), sizeof(int32_t) * rev.size(), cudaMemcpyHostToDevice, st),
@@ -248,7 +256,7 @@ int prepare_adjoint(ct_scn* s) {
                                         ct::adjoint_capacity(s->ctx->device));
   }
   if (!d.lam_state) {
-    int rc = alloc(s, &d.lam_state, plane);
+    int rc = alloc(s, &d.lam_state, plane + 4);  // +4: the adjoint's bulk copies round sizes up to 16 bytes
     if (rc) return rc;
   }
   refresh_delay_bound(s);
@@ -777,10 +785,11 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
       return r__;                        \
     }                                    \
   } while (0)
-  ALLOC(d.gains, S * kGainCols);
-  ALLOC(d.nbr, V * kOffsets);
-  ALLOC(d.coefs, V * kOffsets);
-  ALLOC(d.delays, V * kOffsets);
+  // +4 elements: the adjoint kernel bulk-copies per-tile ranges rounded up to 16 bytes
+  ALLOC(d.gains, S * kGainCols + 4);
+  ALLOC(d.nbr, V * kOffsets + 4);
+  ALLOC(d.coefs, V * kOffsets + 4);
+  ALLOC(d.delays, V * kOffsets + 4);
   ALLOC(d.init_delays, V * kOffsets);
   ALLOC(d.H, B * M * S);
   ALLOC(d.ctrl, S);
@@ -984,7 +993,7 @@ static int run_epoch_impl(ct_scn* scn, int64_t* batch_index, const int32_t* beat
   int rc = derivatives_reset(scn);
   if (rc) return rc;
   if (grad_mode == CT_GRAD_ADJOINT && (!a.freeze_gains || !a.freeze_delays)) {
-    rc = prepare_adjoint(scn);
+    rc = prepare_adjoint(scn, scn->d.rev ? scn->d.ckpt_k : ct::kCkptSteps);
     if (rc) return rc;
   }
   int64_t batch = 0;
@@ -1231,6 +1240,10 @@ int ct_read_profile(ct_scn* scn, double* ms, int64_t* launches) {
 // change from epoch to epoch (Adam bias corrections, batch-metric slots) are
 // read by the kernels from a small device array written before each replay.
 
+// Checkpoint interval of batch members in adjoint mode: segment buffers (2K planes) plus
+// checkpoints (T/K planes) are smallest near K = sqrt(T/2), 22..45 for 1,000..4,000 steps.
+constexpr int kBatchCkptSteps = 64;
+
 struct EpochDev {
   float bias[2];        // 1 - beta1^step, 1 - beta2^step (host powf, as in update.rs:140-141)
   int64_t batch_index;  // batch-wise metric slot
@@ -1390,7 +1403,7 @@ cudaError_t batch_enqueue_epoch(ct_batch* b) {
       al.tiles = fb.tiles;
       al.ntiles = fb.ntiles;
       al.Tmax = fb.Tmax;
-      al.ckpt_steps = ct::kCkptSteps;
+      al.ckpt_steps = kBatchCkptSteps;
       al.status = d0.status;
       al.barrier = d0.barrier;
       B_CUDA(ct::launch_adjoint_tiles(al, std::min(b->adj_grid, fb.ntiles), st));
@@ -1430,7 +1443,7 @@ int batch_prepare(ct_batch* b) {
     ct_scn* s = b->scns[i];
     if (b->grad_mode == CT_GRAD_ADJOINT) {
       const int before = s->d.adj_ring;
-      int rc = prepare_adjoint(s);
+      int rc = prepare_adjoint(s, kBatchCkptSteps);
       if (rc) return rc;
       if (s->d.adj_ring != before) stale = true;
     }

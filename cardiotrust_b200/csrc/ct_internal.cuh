@@ -13,7 +13,7 @@ constexpr int kGainCols = 78;  // 26 offsets x 3 neighbour components
 constexpr int kMaxStepBlock = 8;  // steps advanced between grid barriers in the forward kernel
 constexpr int kFwdTileVoxels = 32;  // voxels per forward tile (consecutive in device order)
 constexpr int kFwdHaloMax = 160;    // largest neighbourhood of a tile the resident forward form stages
-constexpr int kCkptSteps = 256;     // adjoint mode: all-pass state checkpoint interval (power of two)
+constexpr int kCkptSteps = 256;     // adjoint mode: default all-pass checkpoint interval (power of two)
 
 // Device-side grid barrier state: a monotone arrival counter, zeroed before each launch.
 struct GridBarrier {
@@ -73,9 +73,10 @@ struct DeviceScenario {
   int32_t* nhalo;        // [tiles]
   // adjoint mode (ct_adjoint.cu), allocated on first use
   int32_t* rev;          // [V,26] voxel whose offset n points at this voxel, -1 if none
-  float* ckpt;           // [ceil(T/kCkptSteps), V, 78] all-pass state before step s * kCkptSteps
-  float* seg_ap;         // [kCkptSteps, V, 78] recomputed all-pass outputs of one segment
-  float* seg_q;          // [kCkptSteps, V, 78] in_t - ap[t-1] of one segment
+  int ckpt_k;            // checkpoint interval K (power of two)
+  float* ckpt;           // [ceil(T/K), V, 78] all-pass state before step s * K
+  float* seg_ap;         // [min(T, K), pitch] recomputed all-pass outputs of one segment
+  float* seg_q;          // [min(T, K), pitch] in_t - ap[t-1] of one segment
   float* inbox;          // [adj_ring, V, 78] adjoint contributions addressed to (voxel, column) by step
   float* lam_state;      // [V,78] adjoint all-pass state between blocks of steps
   float* dCk;            // [V,78] per-column coefficient-gradient partials
@@ -108,7 +109,8 @@ struct FwdArgs {
   float* ap;
   float* ap_last;
   float* stepsum_part;
-  float* ckpt;  // adjoint checkpoints [ceil(T / kCkptSteps), V, 78] or null
+  float* ckpt;  // adjoint checkpoints [ceil(T / ckpt_k), V, 78] or null
+  int ckpt_k;   // checkpoint interval (power of two)
   const int32_t* dmin;
   float threshold;
   int32_t* status;
@@ -130,7 +132,7 @@ cudaError_t launch_forward_batch(const FwdBatch& b, int grid, cudaStream_t strea
 int forward_batch_capacity(int device);
 
 // Forward propagation of one beat: X[t,:] for t in [0,T). With ckpt non-null the all-pass
-// state before every step s * kCkptSteps (s >= 1) is stored in ckpt[s].
+// state before every step s * d.ckpt_k (s >= 1) is stored in ckpt[s].
 cudaError_t launch_forward(DeviceScenario& d, float threshold, float* ckpt, cudaStream_t stream);
 // CTAs of the streaming form, and how many CTAs of the resident form fit on the device.
 int forward_grid_size(int64_t V, int device);

@@ -141,10 +141,10 @@ __device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int 
   int ck_s = -1;
   float* ck_row = nullptr;
   if (p.ckpt) {
-    const int tc = ((tr0 + kCkptSteps) & ~(kCkptSteps - 1)) - 1;  // first step t >= tr0 with (t+1) % K == 0
+    const int tc = ((tr0 + p.ckpt_k) & ~(p.ckpt_k - 1)) - 1;  // first step t >= tr0 with (t+1) % K == 0
     if (tc < tr0 + R && tc + 1 < p.T) {
       ck_s = tc - tr0;
-      ck_row = p.ckpt + (size_t)((tc + 1) / kCkptSteps) * p.V * kGainCols + (size_t)v0 * kGainCols;
+      ck_row = p.ckpt + (size_t)((tc + 1) / p.ckpt_k) * p.V * kGainCols + (size_t)v0 * kGainCols;
     }
   }
 #pragma unroll
@@ -499,10 +499,10 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
         int ck_s = -1;
         float* ck_row = nullptr;
         if (p.ckpt) {
-          const int tc = ((tr0 + kCkptSteps) & ~(kCkptSteps - 1)) - 1;  // first step t >= tr0 with (t+1) % K == 0
+          const int tc = ((tr0 + p.ckpt_k) & ~(p.ckpt_k - 1)) - 1;  // first step t >= tr0 with (t+1) % K == 0
           if (tc < tr0 + R && tc + 1 < T) {
             ck_s = tc - tr0;
-            ck_row = p.ckpt + (size_t)((tc + 1) / kCkptSteps) * p.V * kGainCols + (size_t)v0 * kGainCols;
+            ck_row = p.ckpt + (size_t)((tc + 1) / p.ckpt_k) * p.V * kGainCols + (size_t)v0 * kGainCols;
           }
         }
 #pragma unroll
@@ -666,6 +666,7 @@ FwdArgs forward_scenario(const DeviceScenario& d, float threshold, float* ckpt, 
   a.ap_last = d.ap_last;
   a.stepsum_part = part;
   a.ckpt = ckpt;
+  a.ckpt_k = d.ckpt_k > 0 ? d.ckpt_k : kCkptSteps;
   a.dmin = d.dmin;
   a.threshold = threshold;
   a.status = d.status;
