@@ -16,10 +16,12 @@
 // Schedule (one cooperative launch per beat, or per beat of a batch of
 // scenarios: every tile names its scenario):
 //   * Checkpoints. The forward stores the all-pass state every K steps
-//     (K a power of two, 256 by default). Segments are visited from the last to the first; a CTA first
-//     recomputes, from the checkpoint and the stored states, ap[t] and
-//     q[t] = in_t - ap[t-1] of its own tiles for the segment (the forward's
-//     fmaf, so bit-identical), then steps the segment backwards.
+//     (K a power of two, 256 by default). Segments are visited from the last
+//     to the first; a CTA first recomputes, from the checkpoint and the
+//     stored states, q[t] = in_t - ap[t-1] of its own tiles for the segment,
+//     then steps the segment backwards, rebuilding ap[t] = fmaf(c, q[t], in1_t)
+//     (the forward's own expression, so bit-identical) from a gather of
+//     in1_t = x[t-d-1, j]: one stored row per step instead of two.
 //   * Inbox. At step t item (v, n) knows lap[t] and lap[t+1], so it writes
 //     w_vn[t-d] into the inbox row of its neighbour j, column 3n+b, slot
 //     (t-d) mod ring. Each inbox cell has exactly one writer and is read at
@@ -27,11 +29,14 @@
 //     at a time between grid barriers, as in the forward. A voxel's 78 inbox
 //     cells are contiguous and summed in column order, so results are
 //     deterministic (no atomics).
-//   * Pipeline. Thread e owns tile columns e, e+512, ... A step's inbox row
-//     and recomputed ap/q rows (contiguous per tile; plane pitch padded to 16
-//     bytes) arrive by TMA bulk copies into a ring of kStages shared-memory
-//     stages, issued kStages steps ahead by one thread and completed on an
-//     mbarrier per stage (every wait bounded); gains sit in shared memory.
+//   * Pipeline. Sixteen threads (half a warp) own one voxel of the tile, five
+//     of its 78 columns each. A step's inbox row and q row (contiguous per
+//     tile; plane pitch padded to 16 bytes) arrive by TMA bulk copies into a
+//     ring of kStages shared-memory stages, issued kStages steps ahead by one
+//     thread and completed on a `full` mbarrier per stage; the states, mapped
+//     residuals and in1 gathers of the step arrive by cp.async. Warps run
+//     decoupled: each releases a stage on an `empty` mbarrier, and no CTA
+//     barrier separates steps. Every wait is bounded.
 //   * A CTA that owns one tile keeps its columns' state and gradient sums in
 //     registers for the launch; otherwise both go through global memory at
 //     the end of every block of steps.
@@ -57,7 +62,7 @@ static_assert(kCols * kGroup >= kGainCols, "columns per voxel");
 
 struct AdjSmem {
   float g[kTileVoxels * 3 * kGainCols];  // the tile's gain rows, [voxel][row a][column k] as in HBM
-  float stage[kStages][3][kTileCols];    // [stage][inbox | ap | q][voxel * 78 + column]
+  float stage[kStages][3][kTileCols];    // [stage][inbox | q | in1][voxel * 78 + column]
   float xm[kStages][kTileVoxels][8];     // [stage][voxel][x0 x1 x2 mr0 mr1 mr2 - -]
   float coef[kTileItems];                // per (voxel, offset) of the tile
   int32_t del[kTileItems];
@@ -149,7 +154,7 @@ __device__ __forceinline__ void load_scn(AdjSmem& sm, const AdjLaunch& L, int sc
 __device__ __forceinline__ int my_voxel() { return threadIdx.x / kGroup; }
 __device__ __forceinline__ int my_col(int i) { return (int)(threadIdx.x % kGroup) + kGroup * i; }
 
-// ap[t] and q[t] = in_t - ap[t-1] of the thread's columns for steps [t_lo, t_hi).
+// q[t] = in_t - ap[t-1] of the thread's columns for steps [t_lo, t_hi).
 __device__ __forceinline__ void recompute_segment(const AdjScn& p, int v0, int nv, int seg, int t_lo, int t_hi) {
   const size_t plane = (size_t)p.V * kGainCols;  // checkpoint planes are unpadded
   const size_t pitch = (size_t)p.pitch;
@@ -190,7 +195,6 @@ __device__ __forceinline__ void recompute_segment(const AdjScn& p, int v0, int n
     for (int u = 0; u < kU; ++u) {
       const int t = t0 + u;
       if (t < t_hi) {
-        float* sa = p.seg_ap + (size_t)(t - t_lo) * pitch + (size_t)(v0 + vl) * kGainCols;
         float* sq = p.seg_q + (size_t)(t - t_lo) * pitch + (size_t)(v0 + vl) * kGainCols;
 #pragma unroll
         for (int i = 0; i < kCols; ++i) {
@@ -198,10 +202,7 @@ __device__ __forceinline__ void recompute_segment(const AdjScn& p, int v0, int n
           const float q = in[u][i] - a[i];
           a[i] = fmaf(c[i], q, inp[i]);
           inp[i] = in[u][i];
-          if (vl < nv && k < kGainCols) {
-            sa[k] = a[i];
-            sq[k] = q;
-          }
+          if (vl < nv && k < kGainCols) sq[k] = q;
         }
       }
     }
@@ -212,6 +213,7 @@ __device__ __forceinline__ void recompute_segment(const AdjScn& p, int v0, int n
 struct Cols {
   float c[kCols], lprev[kCols], dg[kCols][3], dc[kCols];
   int d[kCols], jw[kCols];  // delay; inbox cell neighbour * 78 + column, -1 if unconnected
+  int xo[kCols];            // state index 3 * neighbour + b of the column's input
   uint32_t full_ph;         // bit s: parity of the next completion of full[s]
   uint32_t empty_ph;        // thread 0: parity of the next completion of empty[s]
   uint32_t empty_wait;      // thread 0: bit s: a use of stage s has not been waited empty yet
@@ -245,6 +247,7 @@ __device__ __forceinline__ bool load_cols(Cols& cs, AdjSmem& sm, const AdjScn& p
     cs.c[i] = 0.0f;
     cs.d[i] = 1 << 30;
     cs.jw[i] = -1;
+    cs.xo[i] = 0;
     cs.lprev[i] = 0.0f;
     if (ok && vl < nv && k < kGainCols) {
       const int it = vl * kOffsets + k / 3;
@@ -253,6 +256,7 @@ __device__ __forceinline__ bool load_cols(Cols& cs, AdjSmem& sm, const AdjScn& p
         cs.c[i] = sm.coef[it];
         cs.d[i] = sm.del[it];
         cs.jw[i] = nb * kGainCols + k;
+        cs.xo[i] = 3 * nb + k % 3;
       }
       if (state) cs.lprev[i] = sm.lam[vl * kGainCols + k];
     }
@@ -285,7 +289,7 @@ __device__ __forceinline__ void flush_cols(Cols& cs, const AdjScn& p, int v0, in
   }
 }
 
-// Thread 0: bulk copies of step t's inbox, ap and q rows of the tile into stage `st`, once every
+// Thread 0: bulk copies of step t's inbox and q rows of the tile into stage `st`, once every
 // warp has released the stage's previous use.
 __device__ __forceinline__ bool issue_stage(Cols& cs, AdjSmem& sm, const AdjScn& p, int st, int v0, int nv, int t,
                                            int t_lo, int32_t* status) {
@@ -297,28 +301,37 @@ __device__ __forceinline__ bool issue_stage(Cols& cs, AdjSmem& sm, const AdjScn&
   const size_t pitch = (size_t)p.pitch;
   const uint32_t bytes = (uint32_t)(((nv * kGainCols * 4) + 15) & ~15);  // stays inside the padded row
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  mbar_expect_tx(&sm.full[st], 3 * bytes);
+  mbar_expect_tx(&sm.full[st], 2 * bytes);
   bulk_load(sm.stage[st][0], p.inbox + (size_t)(t & (p.ring - 1)) * pitch + (size_t)v0 * kGainCols, bytes,
             &sm.full[st]);
-  bulk_load(sm.stage[st][1], p.seg_ap + (size_t)(t - t_lo) * pitch + (size_t)v0 * kGainCols, bytes, &sm.full[st]);
-  bulk_load(sm.stage[st][2], p.seg_q + (size_t)(t - t_lo) * pitch + (size_t)v0 * kGainCols, bytes, &sm.full[st]);
+  bulk_load(sm.stage[st][1], p.seg_q + (size_t)(t - t_lo) * pitch + (size_t)v0 * kGainCols, bytes, &sm.full[st]);
   cs.empty_wait |= 1u << st;
   cs.inflight |= 1u << st;
   return true;
 }
 
-// Threads 0-5 of each voxel group: the voxel's states and mapped residuals of step t into stage
-// `st` (one cp.async group per stage and thread, committed even when empty).
-__device__ __forceinline__ void issue_xm(AdjSmem& sm, const AdjScn& p, int st, int v0, int nv, int t, bool real) {
+// Per thread, into stage `st` for step t: threads 0-5 of each voxel group copy the voxel's states
+// and mapped residuals; every thread gathers in1_t = x[t-d-1, j] of its connected columns. One
+// cp.async group per stage and thread, committed even when empty.
+__device__ __forceinline__ void issue_xm(const Cols& cs, AdjSmem& sm, const AdjScn& p, int st, int v0, int nv, int t,
+                                         bool real) {
   const int vl = my_voxel(), q = threadIdx.x % kGroup;
-  if (real && vl < nv && q < 6) {
-    const size_t off = (size_t)t * p.S + 3 * (v0 + vl) + (q % 3);
-    cp_async4(&sm.xm[st][vl][q], (q < 3 ? p.X : p.MR) + off);
+  if (real && vl < nv) {
+    if (q < 6) {
+      const size_t off = (size_t)t * p.S + 3 * (v0 + vl) + (q % 3);
+      cp_async4(&sm.xm[st][vl][q], (q < 3 ? p.X : p.MR) + off);
+    }
+#pragma unroll
+    for (int i = 0; i < kCols; ++i) {
+      const int t1 = t - cs.d[i] - 1;
+      if (cs.jw[i] >= 0 && t1 >= 0)
+        cp_async4(&sm.stage[st][2][vl * kGainCols + my_col(i)], p.X + (size_t)t1 * p.S + cs.xo[i]);
+    }
   }
   cp_async_commit();
 }
 
-// Steps ta down to t_end (inclusive) of one tile; t_lo is the segment's first step (row 0 of seg_ap/seg_q).
+// Steps ta down to t_end (inclusive) of one tile; t_lo is the segment's first step (row 0 of seg_q).
 // Warps run decoupled: a step's rows arrive on full[st], each warp releases them on empty[st].
 // Returns false if a wait timed out (the CTA must leave).
 __device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem& sm, const AdjScn& p, int v0, int nv, int ta,
@@ -335,7 +348,7 @@ __device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem& sm, const AdjS
     for (int s = 0; s < kStages && ta - s >= t_end; ++s)
       if (!issue_stage(cs, sm, p, s, v0, nv, ta - s, t_lo, status)) sm.abort = 1;
   }
-  for (int s = 0; s < kStages; ++s) issue_xm(sm, p, s, v0, nv, ta - s, ta - s >= t_end);
+  for (int s = 0; s < kStages; ++s) issue_xm(cs, sm, p, s, v0, nv, ta - s, ta - s >= t_end);
   for (int t = ta; t >= t_end; --t) {
     const int st = (ta - t) % kStages;
     if (*(volatile int*)&sm.abort) return false;
@@ -387,11 +400,13 @@ __device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem& sm, const AdjS
       if (cs.jw[i] >= 0) {
         const float G = g[k] * lx[0] + g[kGainCols + k] * lx[1] + g[2 * kGainCols + k] * lx[2];
         const float lap = G - cs.c[i] * cs.lprev[i];
-        const float ap_t = sm.stage[st][1][vl * kGainCols + k];
+        const float q_t = sm.stage[st][1][vl * kGainCols + k];
+        const float in1 = t - cs.d[i] - 1 >= 0 ? sm.stage[st][2][vl * kGainCols + k] : 0.0f;
+        const float ap_t = fmaf(cs.c[i], q_t, in1);  // the forward's all-pass output at step t
         cs.dg[i][0] = cs.dg[i][0] + lx[0] * ap_t;
         cs.dg[i][1] = cs.dg[i][1] + lx[1] * ap_t;
         cs.dg[i][2] = cs.dg[i][2] + lx[2] * ap_t;
-        cs.dc[i] = cs.dc[i] + lap * sm.stage[st][2][vl * kGainCols + k];
+        cs.dc[i] = cs.dc[i] + lap * q_t;
         const int ts = t - cs.d[i];
         if (ts >= 0) p.inbox[(size_t)(ts & rmask) * pitch + cs.jw[i]] = cs.c[i] * lap + cs.lprev[i];
         cs.lprev[i] = lap;
@@ -399,7 +414,7 @@ __device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem& sm, const AdjS
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty[st]);
-    issue_xm(sm, p, st, v0, nv, t - kStages, t - kStages >= t_end);
+    issue_xm(cs, sm, p, st, v0, nv, t - kStages, t - kStages >= t_end);
     if (threadIdx.x == 0 && t - kStages >= t_end)
       if (!issue_stage(cs, sm, p, st, v0, nv, t - kStages, t_lo, status)) sm.abort = 1;
   }
@@ -570,7 +585,6 @@ AdjScn adjoint_scenario(const DeviceScenario& d, const AdjointScalars& s) {
   a.X = d.X;
   a.MR = d.MR;
   a.ckpt = d.ckpt;
-  a.seg_ap = d.seg_ap;
   a.seg_q = d.seg_q;
   a.inbox = d.inbox;
   a.lam_state = d.lam_state;

@@ -216,9 +216,9 @@ int prepare_adjoint(ct_scn* s, int k = ct::kCkptSteps) {
   const int64_t V = d.V, plane = d.V * kGainCols;
   if (d.rev && d.ckpt_k != k) {  // re-made below with the new interval
     CT_CUDA(cudaStreamSynchronize(st), "adjoint re-layout");
-    for (void* p : {(void*)d.rev, (void*)d.ckpt, (void*)d.seg_ap, (void*)d.seg_q}) release(s, p);
+    for (void* p : {(void*)d.rev, (void*)d.ckpt, (void*)d.seg_q}) release(s, p);
     d.rev = nullptr;
-    d.ckpt = d.seg_ap = d.seg_q = nullptr;
+    d.ckpt = d.seg_q = nullptr;
   }
   if (!d.rev) {
     std::vector<int32_t> rev((size_t)(V * kOffsets), -1);
@@ -238,13 +238,12 @@ int prepare_adjoint(ct_scn* s, int k = ct::kCkptSteps) {
     d.ckpt_k = k;
     int rc = alloc(s, &d.rev, V * kOffsets);
     if (!rc) rc = alloc(s, &d.ckpt, nseg * plane);
-    if (!rc) rc = alloc(s, &d.seg_ap, seg_steps * d.adj_pitch);
     if (!rc) rc = alloc(s, &d.seg_q, seg_steps * d.adj_pitch);
     if (!rc && !d.dCk) rc = alloc(s, &d.dCk, plane);
     if (rc) {
-      for (void* p : {(void*)d.rev, (void*)d.ckpt, (void*)d.seg_ap, (void*)d.seg_q}) release(s, p);
+      for (void* p : {(void*)d.rev, (void*)d.ckpt, (void*)d.seg_q}) release(s, p);
       d.rev = nullptr;
-      d.ckpt = d.seg_ap = d.seg_q = nullptr;
+      d.ckpt = d.seg_q = nullptr;
       return rc;
     }
     CT_CUDA(cudaMemcpyAsync(d.rev, rev.data(), sizeof(int32_t) * rev.size(), cudaMemcpyHostToDevice, st),

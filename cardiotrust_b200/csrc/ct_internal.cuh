@@ -75,13 +75,12 @@ struct DeviceScenario {
   int32_t* rev;          // [V,26] voxel whose offset n points at this voxel, -1 if none
   int ckpt_k;            // checkpoint interval K (power of two)
   float* ckpt;           // [ceil(T/K), V, 78] all-pass state before step s * K
-  float* seg_ap;         // [min(T, K), pitch] recomputed all-pass outputs of one segment
   float* seg_q;          // [min(T, K), pitch] in_t - ap[t-1] of one segment
   float* inbox;          // [adj_ring, V, 78] adjoint contributions addressed to (voxel, column) by step
   float* lam_state;      // [V,78] adjoint all-pass state between blocks of steps
   float* dCk;            // [V,78] per-column coefficient-gradient partials
   int adj_ring;          // inbox slots (power of two)
-  int adj_pitch;         // floats per plane of seg_ap, seg_q and inbox: V * 78 rounded up to 4 (16-byte rows)
+  int adj_pitch;         // floats per plane of seg_q and inbox: V * 78 rounded up to 4 (16-byte rows)
   int adj_grid;          // CTAs of the adjoint kernel
   // plain form (ct_plain.cu), allocated on first use
   float* plain_mreg;     // [S] maximum regularisation of the current step
@@ -168,7 +167,7 @@ struct AdjointScalars {
 // One scenario as the adjoint kernel sees it (device pointers, sizes, scalars).
 struct AdjScn {
   int V, S, T, ring;
-  int pitch;  // floats between consecutive planes of seg_ap, seg_q and inbox (V * 78 rounded up to 4)
+  int pitch;  // floats between consecutive planes of seg_q and inbox (V * 78 rounded up to 4)
   const int32_t* nbr;
   const float* coefs;
   const int32_t* delays;
@@ -177,7 +176,6 @@ struct AdjScn {
   const float* X;
   const float* MR;
   const float* ckpt;
-  float* seg_ap;
   float* seg_q;
   float* inbox;
   float* lam_state;
