@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--batch-scenarios", type=int, default=64,
                    help="scenarios of the batched section (0 skips it)")
     p.add_argument("--batch-epochs", type=int, default=3, help="timed epochs of the batched section")
+    p.add_argument("--precision-steps", type=int, default=48,
+                   help="steps of the precision report (shell, 256 triaxial sensors) against the f64 oracle (0 skips)")
     return p.parse_args()
 
 
@@ -327,6 +329,93 @@ def batched_section(args, alg, sc, ctx, prec, stream, flush):
     }
 
 
+def precision_reference(steps):
+    """The precision report's workload and its f64 oracle results (run on the host, in a thread).
+
+    The precision config (the 64x64x48 shell, 256 triaxial sensors = 768 rows, 1 % noise) with its
+    beat cut to `steps` steps, so that the f64 CPU oracle finishes in tens of seconds; ground truth
+    from the f32 oracle forward. Returns (scenario, {name: f64 result}) of one reference-mode epoch and
+    of the adjoint gradient, both from the pre-update parameters."""
+    import numpy as np
+
+    import oracle
+    from cardiotrust_b200 import scenario as sc
+
+    spec = sc.workload_spec("shell_precision")
+    spec.num_steps = steps
+    scn = sc.build(spec)
+    t = scn.truth
+    fwd = oracle.OracleEpoch(t.gains, t.output_state_indices, t.coefs, t.delays, t.initial_delays,
+                             scn.measurement_matrix, scn.control_matrix, scn.control_function)
+    y = fwd.simulate().astype(np.float64)
+    del fwd
+    rng = np.random.default_rng(spec.seed + 7919)  # 1 % noise, as the precision config specifies
+    sigma = spec.noise_fraction * float(np.sqrt(np.mean(y ** 2)))
+    scn.measurements = (y + rng.normal(0.0, sigma, size=y.shape)).astype(np.float32)
+    a = oracle.algo(optimizer=1, learning_rate=1e-3, freeze_delays=0)
+    ref = oracle.from_scenario(scn, dtype=np.float64)
+    ref.run_epoch(a)
+    out = {"system_states": ref.system_states.copy(), "measurements": ref.measurements.copy(),
+           "residuals": ref.residuals.copy(), "grad_gains": ref.d_gains.copy(), "grad_coefs": ref.d_coefs.copy()}
+    del ref
+    adj = oracle.from_scenario(scn, dtype=np.float64)
+    adj.stated_loss(a, gradient=True)
+    out["adjoint_grad_gains"] = adj.d_gains.copy()
+    out["adjoint_grad_coefs"] = adj.d_coefs.copy()
+    return scn, out
+
+
+def precision_section(alg, ctx, job):
+    """Relative error (norm-wise, f64) of every result of each product precision against the f64 oracle."""
+    import numpy as np
+
+    job.join()
+    if job.error is not None:
+        return {"error": repr(job.error)}
+    scn, ref = job.result
+    cfg = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
+
+    def rel(a, b):
+        a = np.asarray(a, np.float64)
+        b = np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    results = {}
+    for name, prec in (("fp32", alg.Precision.Fp32), ("tf32x3", alg.Precision.Tf32x3), ("tf32", alg.Precision.Tf32)):
+        eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=cfg)
+        eng.run_epoch(0, beat_order=np.arange(scn.num_beats), precision=prec)
+        r = {f: rel(eng.read(f), ref[f]) for f in ("system_states", "measurements", "residuals", "grad_gains",
+                                                   "grad_coefs")}
+        eng.close()
+        eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=cfg)
+        eng.run_epoch(0, beat_order=np.arange(scn.num_beats), grad_mode=alg.GradMode.Adjoint, precision=prec)
+        r["adjoint_grad_gains"] = rel(eng.read("grad_gains"), ref["adjoint_grad_gains"])
+        r["adjoint_grad_coefs"] = rel(eng.read("grad_coefs"), ref["adjoint_grad_coefs"])
+        eng.close()
+        results[name] = r
+    return {
+        "workload": f"64x64x48 shell ({scn.num_voxels} voxels, {scn.num_states} states), {scn.num_sensors} sensor "
+                    f"rows (256 triaxial sensors), beat cut to {scn.num_steps} steps so the f64 CPU oracle finishes; "
+                    "Adam, gains+coefficients",
+        "error": "||gpu - f64 oracle|| / ||f64 oracle|| per result (states [T,S], measurements [T,M], last-step "
+                 "residuals, reference-mode and adjoint gradients)",
+        "targets": {"states": 1e-4, "gradients": 1e-3},
+        "results": results,
+    }
+
+
+class _Job(threading.Thread):
+    def __init__(self, fn, *a):
+        super().__init__(daemon=True)
+        self.fn, self.a, self.result, self.error = fn, a, None, None
+
+    def run(self):
+        try:
+            self.result = self.fn(*self.a)
+        except Exception as exc:  # reported in the JSON line, never fatal
+            self.error = exc
+
+
 def gpu_arm(args):
     import numpy as np
     import torch
@@ -342,6 +431,12 @@ def gpu_arm(args):
                                 device_id=torch.device("cuda", local_rank))
     from cardiotrust_b200 import algorithm as alg
     from cardiotrust_b200 import scenario as sc
+
+    # the precision report's f64 oracle runs on the host while the GPU sections run
+    prec_job = None
+    if args.precision_steps > 0 and rank == 0 and world == 1:
+        prec_job = _Job(precision_reference, args.precision_steps)
+        prec_job.start()
 
     # a dedicated stream: the library issues every kernel on it, and the timing events,
     # the L2 flush and the barriers below are ordered on it too
@@ -461,6 +556,8 @@ def gpu_arm(args):
         eng.close()
         batched = batched_section(args, alg, sc, ctx, prec, stream, flush)
 
+    precision = precision_section(alg, ctx, prec_job) if prec_job is not None else None
+
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
     if rank == 0 and world == 1:
@@ -508,6 +605,7 @@ def gpu_arm(args):
             "forms": forms,
             "chosen_vs_plain": value / forms["plain"]["scenario_epochs_per_s"],
             "batched": batched,
+            "precision": precision,
         }
         print(json.dumps(line), flush=True)
     eng.close()

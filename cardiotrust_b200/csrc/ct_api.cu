@@ -974,7 +974,8 @@ static int run_epoch_impl(ct_scn* scn, int64_t* batch_index, const int32_t* beat
   if (precision != CT_PREC_FP32 && precision != CT_PREC_TF32X3 && precision != CT_PREC_TF32)
     return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
   if (precision != CT_PREC_FP32 && !scn->d.umma)
-    return fail(CT_ERR_NOT_SUPPORTED, "tensor-core precision needs num_states divisible by 4 (16-byte TMA rows)");
+    return fail(CT_ERR_NOT_SUPPORTED,
+                "tensor-core precision needs num_states divisible by 4 (16-byte TMA rows) and the driver's TMA encoder");
   CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
   DeviceScenario& d = scn->d;
   const ct_algorithm& a = scn->algo;

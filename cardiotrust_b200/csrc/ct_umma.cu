@@ -440,7 +440,8 @@ cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& a_lo, const CUt
 
 // ---- public launchers (ct_internal.cuh)
 
-bool umma_supported(int64_t S, int64_t M) { return (S % 4) == 0 && M <= 256 && encode_fn() != nullptr; }
+// Rows of X and H^T need 16-byte strides (S % 4 == 0); sensor rows beyond 256 take more column tiles of H x.
+bool umma_supported(int64_t S, int64_t M) { return (S % 4) == 0 && M <= 65536 && encode_fn() != nullptr; }
 
 int umma_yn(int64_t M) { return M <= 128 ? 128 : 256; }
 

@@ -331,6 +331,27 @@ def test_tensor_core_shapes(alg, ctx, oracle_mod):
         eng.close()
 
 
+def test_tensor_core_many_sensor_rows(alg, ctx, oracle_mod):
+    """256 triaxial sensors (768 rows, as in the precision config): H x takes three 256-column tiles."""
+    from cardiotrust_b200 import scenario as sc
+
+    spec = sc.ScenarioSpec(shape=(6, 5, 4), num_steps=140, num_sensors=256, patho_size=2, patho_origin=(2, 2, 1),
+                           pulse_onset=1, pulse_sigma_samples=4.0, noise_fraction=0.01, seed=12)
+    scn = sc.attach_measurements(sc.build(spec), oracle_forward(oracle_mod))
+    assert scn.num_sensors == 768 and scn.num_states % 4 == 0
+    a, oa = algo_pair(alg, oracle_mod, optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
+    o64 = oracle_mod.from_scenario(scn, dtype=np.float64)
+    o64.run_epoch(oa)
+    for precision in (alg.Precision.Tf32x3, alg.Precision.Tf32):
+        eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=a)
+        eng.run_epoch(0, precision=precision)
+        loose = precision == alg.Precision.Tf32
+        assert rel_err(eng.read("measurements"), o64.measurements) < (5e-4 if loose else TOL_MEAS), precision
+        assert rel_err(eng.read("mapped_residuals_history"), _mr_history(o64, scn)) < (5e-3 if loose else 1e-4)
+        assert rel_err(eng.read("grad_gains"), o64.d_gains) < (5e-3 if loose else TOL_GRAD), precision
+        eng.close()
+
+
 def _mr_history(o64, scn):
     """H^T r of every step of the last beat, in float64, from the oracle's residuals."""
     H = scn.measurement_matrix[-1].astype(np.float64)
