@@ -329,19 +329,20 @@ def batched_section(args, alg, sc, ctx, prec, stream, flush):
     }
 
 
-def precision_reference(steps):
-    """The precision report's workload and its f64 oracle results (run on the host, in a thread).
+def precision_reference(workload, steps):
+    """One precision-report case and its f64 oracle results (run on the host, in a thread).
 
-    The precision config (the 64x64x48 shell, 256 triaxial sensors = 768 rows, 1 % noise) with its
-    beat cut to `steps` steps, so that the f64 CPU oracle finishes in tens of seconds; ground truth
-    from the f32 oracle forward. Returns (scenario, {name: f64 result}) of one reference-mode epoch and
-    of the adjoint gradient, both from the pre-update parameters."""
+    The workload (the precision config: the 64x64x48 shell with 256 triaxial sensors = 768 rows; or
+    the headline cuboid) with its beat cut to `steps` steps, so that the f64 CPU oracle finishes in
+    tens of seconds; ground truth from the f32 oracle forward plus the workload's 1 % noise. Returns
+    (scenario, {name: f64 result}) of one reference-mode epoch and of the adjoint gradient, both from
+    the pre-update parameters."""
     import numpy as np
 
     import oracle
     from cardiotrust_b200 import scenario as sc
 
-    spec = sc.workload_spec("shell_precision")
+    spec = sc.workload_spec(workload)
     spec.num_steps = steps
     scn = sc.build(spec)
     t = scn.truth
@@ -365,14 +366,29 @@ def precision_reference(steps):
     return scn, out
 
 
+PRECISION_CASES = (("shell_precision", None), ("cuboid20", 400))
+
+
+def precision_cases(steps):
+    return [precision_reference(w, steps if n is None else n) for w, n in PRECISION_CASES]
+
+
 def precision_section(alg, ctx, job):
     """Relative error (norm-wise, f64) of every result of each product precision against the f64 oracle."""
-    import numpy as np
-
     job.join()
     if job.error is not None:
         return {"error": repr(job.error)}
-    scn, ref = job.result
+    out = {"error": "||gpu - f64 oracle|| / ||f64 oracle|| per result (states [T,S], measurements [T,M], last-step "
+                    "residuals, reference-mode and adjoint gradients)",
+           "targets": {"states": 1e-4, "gradients": 1e-3}, "cases": []}
+    for scn, ref in job.result:
+        out["cases"].append(precision_case(alg, ctx, scn, ref))
+    return out
+
+
+def precision_case(alg, ctx, scn, ref):
+    import numpy as np
+
     cfg = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
 
     def rel(a, b):
@@ -394,12 +410,9 @@ def precision_section(alg, ctx, job):
         eng.close()
         results[name] = r
     return {
-        "workload": f"64x64x48 shell ({scn.num_voxels} voxels, {scn.num_states} states), {scn.num_sensors} sensor "
-                    f"rows (256 triaxial sensors), beat cut to {scn.num_steps} steps so the f64 CPU oracle finishes; "
-                    "Adam, gains+coefficients",
-        "error": "||gpu - f64 oracle|| / ||f64 oracle|| per result (states [T,S], measurements [T,M], last-step "
-                 "residuals, reference-mode and adjoint gradients)",
-        "targets": {"states": 1e-4, "gradients": 1e-3},
+        "workload": f"{scn.spec.mask} {scn.spec.shape} ({scn.num_voxels} voxels, {scn.num_states} states), "
+                    f"{scn.num_sensors} sensor rows, beat cut to {scn.num_steps} steps so the f64 CPU oracle "
+                    "finishes; 1 % noise; Adam, gains+coefficients",
         "results": results,
     }
 
@@ -435,7 +448,7 @@ def gpu_arm(args):
     # the precision report's f64 oracle runs on the host while the GPU sections run
     prec_job = None
     if args.precision_steps > 0 and rank == 0 and world == 1:
-        prec_job = _Job(precision_reference, args.precision_steps)
+        prec_job = _Job(precision_cases, args.precision_steps)
         prec_job.start()
 
     # a dedicated stream: the library issues every kernel on it, and the timing events,

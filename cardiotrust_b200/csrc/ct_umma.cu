@@ -4,9 +4,13 @@
 //
 // Both run as TF32 MMAs (kind::tf32, FP32 accumulation in tensor memory) fed
 // by TMA with 128-byte swizzled K-major tiles. Precision modes:
-//   * TF32x3: every operand is split into hi = rna_tf32(v) and lo = v - hi
-//     and the product accumulates hi*hi + hi*lo + lo*hi (the lo*lo term,
-//     ~2^-22 relative, is dropped), which keeps FP32-level accuracy;
+//   * TF32x3: every operand is split into hi = rna_tf32(v) and
+//     lo = rna_tf32(v - hi) and the product accumulates hi*hi + hi*lo + lo*hi
+//     (the lo*lo term, ~2^-22 relative, is dropped). Rounding lo to TF32
+//     before the MMA matters: the tensor core would otherwise truncate it,
+//     a biased 2^-21 error per product that accumulates over the steps of a
+//     gradient when the residuals are small; rounded, the error is unbiased
+//     and ~2^-22, close to FP32 products;
 //   * TF32: one pass, hi*hi.
 // H (and its transpose) are split once per scenario; the residuals are split
 // by the reduction that produces them; the state history is split in shared
@@ -32,6 +36,11 @@ namespace ct {
 namespace {
 
 constexpr int kBM = 128;          // output rows per tile (tensor-memory lanes)
+// K chunks accumulated in tensor memory before the epilogue adds them into the promoted FP32 sum.
+// The tensor core's accumulation over long chains drifts (its adds are not round-to-nearest);
+// promoting every few chunks keeps the product at FP32 quality (measured on the 768-row
+// precision config: relative error of H x 6e-6 without promotion, FP32-level with it).
+constexpr int kPromote = 8;
 constexpr int kBK = 32;           // K elements per chunk (one 128-byte swizzle row of f32)
 constexpr int kUmmaK = 8;         // K per tf32 MMA instruction
 constexpr int kThreadsUmma = 192;  // 6 warps
@@ -134,6 +143,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16};" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+      "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+      "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+
 __device__ __forceinline__ float tf32_rna(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -158,14 +178,17 @@ __global__ void __launch_bounds__(kThreadsUmma, 1)
                      int chunks_per_split, int32_t* status) {
   using L = UmmaSmem<NT, PASSES, SPLIT_A>;
   constexpr int kStages = L::kStages;
-  constexpr int kTmemCols = NT <= 32 ? 32 : (NT <= 64 ? 64 : (NT <= 128 ? 128 : 256));
+  // tensor memory: the group accumulator (columns [0, kAccCols)) and the promoted sum ([kAccCols, 2 kAccCols))
+  constexpr int kAccCols = NT <= 32 ? 32 : (NT <= 64 ? 64 : (NT <= 128 ? 128 : 256));
+  constexpr int kTmemCols = 2 * kAccCols;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + kStages * L::kStageBytes);
   uint64_t* conv = full + kStages;
   uint64_t* empty = conv + kStages;
-  uint64_t* accum = empty + kStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
+  uint64_t* accum = empty + kStages;  // a group of K chunks is complete in the accumulator
+  uint64_t* acc_empty = accum + 1;    // the epilogue warps have promoted the group
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -186,6 +209,7 @@ __global__ void __launch_bounds__(kThreadsUmma, 1)
       mbar_init(&empty[s], 1);
     }
     mbar_init(accum, 1);
+    mbar_init(acc_empty, 4);  // one arrival per epilogue warp
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -230,6 +254,12 @@ __global__ void __launch_bounds__(kThreadsUmma, 1)
       for (int i = 0; i < nchunks && ok; ++i) {
         const int s = i % kStages;
         const uint32_t ph = (i / kStages) & 1;
+        const int g = i / kPromote;
+        const bool first = (i % kPromote) == 0;
+        if (first && g > 0) {  // the accumulator is free once the previous group is promoted
+          if (!mbar_wait(acc_empty, (g - 1) & 1, status, abort_flag)) break;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        }
         ok = SPLIT_A ? mbar_wait(&conv[s], ph, status, abort_flag) : mbar_wait(&full[s], ph, status, abort_flag);
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -240,7 +270,7 @@ __global__ void __launch_bounds__(kThreadsUmma, 1)
 #pragma unroll
         for (int kk = 0; kk < kBK / kUmmaK; ++kk) {
           const uint64_t off = (uint64_t)(kk * kUmmaK * 4) >> 4;  // K step inside the swizzle row
-          const uint32_t acc = (i > 0 || kk > 0) ? 1u : 0u;
+          const uint32_t acc = (first && kk == 0) ? 0u : 1u;
           umma_tf32(tmem, dah + off, dbh + off, idesc, acc);
           if (PASSES == 3) {
             umma_tf32(tmem, dah + off, dbl + off, idesc, 1u);
@@ -248,17 +278,69 @@ __global__ void __launch_bounds__(kThreadsUmma, 1)
           }
         }
         umma_commit(&empty[s]);  // frees the stage once these MMAs have read it
+        if ((i % kPromote) == kPromote - 1 || i == nchunks - 1) umma_commit(accum);  // group complete
       }
-      umma_commit(accum);  // accumulator complete (arrives after all MMAs issued above)
     }
   } else {
     // ---- converter / epilogue warps 2..5 (128 threads)
     const int ct = threadIdx.x - 64;
+    const int quarter = warp % 4;  // tensor-memory lanes 32*quarter .. +31
+    const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+    const int r = quarter * 32 + lane;
+    const int gm = m0 + r;
+    float* crow = C + (long long)blockIdx.z * c_split_stride + (long long)gm * ldc;
+    const int ngroups = (nchunks + kPromote - 1) / kPromote;
+    auto store16 = [&](int c0, const float* v) {
+      if (gm < rows) {
+        if (n0 + c0 + 16 <= cols && ((ldc & 3) == 0)) {
+          float4* dst = reinterpret_cast<float4*>(crow + n0 + c0);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (n0 + c0 + j < cols) crow[n0 + c0 + j] = v[j];
+        }
+      }
+    };
+    // Promotion of group g: promoted += accumulator (FP32 adds, round to nearest, in group order);
+    // the last group goes to global memory instead.
+    auto promote = [&](int g) -> bool {
+      if (!mbar_wait(accum, (uint32_t)(g & 1), status, abort_flag)) return false;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const bool last = g == ngroups - 1;
+#pragma unroll 1
+      for (int c0 = 0; c0 < NT; c0 += 16) {
+        float a[16];
+        tmem_ld16(lane_base + (uint32_t)c0, a);
+        if (g > 0) {
+          float p[16];
+          tmem_ld16(lane_base + (uint32_t)(kAccCols + c0), p);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) a[j] = p[j] + a[j];
+        }
+        if (last)
+          store16(c0, a);
+        else
+          tmem_st16(lane_base + (uint32_t)(kAccCols + c0), a);
+      }
+      if (!last) {
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acc_empty);
+      }
+      return true;
+    };
+    bool ok = true;
     if (SPLIT_A) {
-      for (int i = 0; i < nchunks; ++i) {
+      for (int i = 0; i < nchunks && ok; ++i) {
         const int s = i % kStages;
         const uint32_t ph = (i / kStages) & 1;
-        if (!mbar_wait(&full[s], ph, status, abort_flag)) break;
+        if (!mbar_wait(&full[s], ph, status, abort_flag)) {
+          ok = false;
+          break;
+        }
         float4* hi = reinterpret_cast<float4*>(a_hi(s));
         float4* lo = reinterpret_cast<float4*>(a_lo(s));
 #pragma unroll
@@ -272,47 +354,27 @@ __global__ void __launch_bounds__(kThreadsUmma, 1)
           h.w = tf32_rna(v.w);
           hi[e] = h;
           if (PASSES == 3) {
-            l.x = v.x - h.x;
-            l.y = v.y - h.y;
-            l.z = v.z - h.z;
-            l.w = v.w - h.w;
+            l.x = tf32_rna(v.x - h.x);
+            l.y = tf32_rna(v.y - h.y);
+            l.z = tf32_rna(v.z - h.z);
+            l.w = tf32_rna(v.w - h.w);
             lo[e] = l;
           }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // make the stores visible to the MMA
         __syncwarp();
         if (lane == 0) mbar_arrive(&conv[s]);
+        // the group this chunk closes has no conversion left; promote it as soon as its MMAs finish
+        if ((i % kPromote) == kPromote - 1 || i == nchunks - 1) ok = promote(i / kPromote);
       }
+    } else {
+      for (int g = 0; g < ngroups && ok; ++g) ok = promote(g);
     }
-    // epilogue: tensor memory -> registers -> global
-    const bool have = mbar_wait(accum, 0, status, abort_flag);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (have) {
-      const int quarter = warp % 4;  // tensor-memory lanes 32*quarter .. +31
-      const int r = quarter * 32 + lane;
-      const int gm = m0 + r;
-      float* crow = C + (long long)blockIdx.z * c_split_stride + (long long)gm * ldc;
-#pragma unroll 1
-      for (int c0 = 0; c0 < NT; c0 += 16) {
-        float v[16];
-        if (nchunks > 0) {
-          tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, v);
-        } else {  // a split without K chunks contributes zeros to the fixed-order reduction
+    if (ngroups == 0) {  // a split without K chunks contributes zeros to the fixed-order reduction
+      float z[16];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) v[j] = 0.0f;
-        }
-        if (gm < rows) {
-          if (n0 + c0 + 16 <= cols && ((ldc & 3) == 0)) {
-            float4* dst = reinterpret_cast<float4*>(crow + n0 + c0);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-          } else {
-#pragma unroll
-            for (int j = 0; j < 16; ++j)
-              if (n0 + c0 + j < cols) crow[n0 + c0 + j] = v[j];
-          }
-        }
-      }
+      for (int j = 0; j < 16; ++j) z[j] = 0.0f;
+      for (int c0 = 0; c0 < NT; c0 += 16) store16(c0, z);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -332,7 +394,7 @@ __global__ void split_tf32_kernel(const float* __restrict__ src, float* __restri
   const float v = src[i];
   const float h = tf32_rna(v);
   hi[i] = h;
-  lo[i] = v - h;
+  lo[i] = tf32_rna(v - h);
 }
 
 // Ht[b][s][k] = split(H[b][k][s]) for k < M, zero for M <= k < kpad.
@@ -354,7 +416,7 @@ __global__ void transpose_split_kernel(const float* __restrict__ H, int M, int S
       const float h = tf32_rna(v);
       const long long o = ((long long)b * S + s) * kpad + k;
       hi[o] = h;
-      lo[o] = v - h;
+      lo[o] = tf32_rna(v - h);
     }
   }
 }
@@ -379,7 +441,7 @@ __global__ void reduce_split_kernel(const float* __restrict__ part, int ksplit, 
   if (r_hi) {
     const float h = tf32_rna(r);
     r_hi[idx] = h;
-    r_lo[idx] = r - h;
+    r_lo[idx] = tf32_rna(r - h);
   }
 }
 
