@@ -80,6 +80,8 @@ EXPORTED = [
     "ct_batch_run_epoch",
     "ct_batch_sync",
     "ct_batch_info",
+    "ct_batch_set_profiling",
+    "ct_batch_read_profile",
     "ct_simulate",
     "ct_set_algorithm",
     "ct_set_freeze",
@@ -169,6 +171,8 @@ def load(path: pathlib.Path = LIB_PATH) -> ctypes.CDLL:
     lib.ct_batch_run_epoch.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     lib.ct_batch_sync.argtypes = [vp]
     lib.ct_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int)]
+    lib.ct_batch_set_profiling.argtypes = [vp, ctypes.c_int]
+    lib.ct_batch_read_profile.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.ct_simulate.argtypes = [vp, _fp, _fp]
     lib.ct_set_algorithm.argtypes = [vp, ctypes.POINTER(CtAlgorithm)]
     lib.ct_set_freeze.argtypes = [vp, ctypes.c_int, ctypes.c_int]

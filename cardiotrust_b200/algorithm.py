@@ -344,6 +344,15 @@ class EpochBatch:
         check(lib().ct_batch_info(self._h, ctypes.byref(k), ctypes.byref(g)))
         return {"graph_kernels": int(k.value), "uses_graph": bool(g.value)}
 
+    def set_profiling(self, enable: bool) -> None:
+        """Per-phase CUDA-event timing of batched epochs (eager launches while enabled)."""
+        check(lib().ct_batch_set_profiling(self._h, int(enable)))
+
+    def read_profile(self) -> dict:
+        ms = (ctypes.c_double * len(_lib.PHASES))()
+        check(lib().ct_batch_read_profile(self._h, ms))
+        return {name: float(ms[i]) for i, name in enumerate(_lib.PHASES)}
+
     def close(self) -> None:
         if self._h:
             lib().ct_batch_destroy(self._h)

@@ -1273,6 +1273,11 @@ struct ct_batch {
   std::vector<int> captured_ring;
   std::vector<uint64_t> captured_gen;
   int64_t graph_kernels = 0;
+  // optional per-phase timing (eager launches, CUDA events on the context stream)
+  bool profiling = false;
+  cudaEvent_t open_event = nullptr;
+  std::vector<PhaseEvents> pending;
+  double phase_ms[CT_PHASE_COUNT] = {};
 };
 
 namespace {
@@ -1285,6 +1290,13 @@ int batch_alloc(ct_batch* b, void** p, size_t bytes) {
 }
 
 void batch_free(ct_batch* b) {
+  for (auto& pe : b->pending) {
+    cudaEventDestroy(pe.start);
+    cudaEventDestroy(pe.stop);
+  }
+  b->pending.clear();
+  if (b->open_event) cudaEventDestroy(b->open_event);
+  b->open_event = nullptr;
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
@@ -1325,10 +1337,33 @@ cudaError_t join_side(ct_batch* b) {
     if (e__ != cudaSuccess) return e__;      \
   } while (0)
 
+// Profiling: closes the phase opened by the previous mark (closes_phase >= 0) and opens the next one.
+// Every event belongs to exactly one (start, stop) pair.
+cudaError_t batch_mark(ct_batch* b, int closes_phase) {
+  if (!b->profiling) return cudaSuccess;
+  cudaStream_t st = b->ctx->stream;
+  cudaError_t err;
+  if (b->open_event && closes_phase >= 0) {
+    cudaEvent_t stop = nullptr;
+    if ((err = cudaEventCreate(&stop)) != cudaSuccess) return err;
+    if ((err = cudaEventRecord(stop, st)) != cudaSuccess) return err;
+    b->pending.push_back({closes_phase, b->open_event, stop});
+  } else if (b->open_event) {
+    cudaEventDestroy(b->open_event);
+  }
+  b->open_event = nullptr;
+  cudaEvent_t start = nullptr;
+  if ((err = cudaEventCreate(&start)) != cudaSuccess) return err;
+  if ((err = cudaEventRecord(start, st)) != cudaSuccess) return err;
+  b->open_event = start;
+  return cudaSuccess;
+}
+
 // Everything of one epoch, enqueued on the context stream and the side streams.
 cudaError_t batch_enqueue_epoch(ct_batch* b) {
   cudaStream_t st = b->ctx->stream;
   const size_t n = b->scns.size();
+  B_CUDA(batch_mark(b, -1));
   auto side_of = [&](size_t i) { return b->side[i % b->side.size()]; };
   const bool adjoint = b->grad_mode == CT_GRAD_ADJOINT;
   // Derivatives::reset of every scenario
@@ -1367,6 +1402,7 @@ cudaError_t batch_enqueue_epoch(ct_batch* b) {
     fb.status = d0.status;
     fb.barrier = d0.barrier;
     B_CUDA(ct::launch_forward_batch(fb, std::min(b->fwd_grid, fb.ntiles), st));
+    B_CUDA(batch_mark(b, CT_PHASE_FORWARD));
     // measurement products, residuals, (reference) derivations and step metrics per scenario
     B_CUDA(fork_side(b));
     for (size_t i = 0; i < n; ++i) {
@@ -1375,7 +1411,8 @@ cudaError_t batch_enqueue_epoch(ct_batch* b) {
       if (beat >= d.B) continue;
       cudaStream_t ss = side_of(i);
       const ct_algorithm& a = s->algo;
-      if (b->precision == CT_PREC_FP32) {
+      // members whose states cannot be tensor-mapped (num_states not a multiple of 4) use FP32 products
+      if (b->precision == CT_PREC_FP32 || !d.umma) {
         B_CUDA(ct::launch_measure(d, beat, true, ss));
         B_CUDA(ct::launch_map_residuals(d, beat, ss));
       } else {
@@ -1406,7 +1443,11 @@ cudaError_t batch_enqueue_epoch(ct_batch* b) {
       al.ckpt_steps = kBatchCkptSteps;
       al.status = d0.status;
       al.barrier = d0.barrier;
+      B_CUDA(batch_mark(b, CT_PHASE_MEASURE));
       B_CUDA(ct::launch_adjoint_tiles(al, std::min(b->adj_grid, fb.ntiles), st));
+      B_CUDA(batch_mark(b, CT_PHASE_DERIVE));
+    } else {
+      B_CUDA(batch_mark(b, CT_PHASE_MEASURE));
     }
   }
   // calculate_average_delays -> batch derivatives -> update -> batch metrics, per scenario
@@ -1431,6 +1472,7 @@ cudaError_t batch_enqueue_epoch(ct_batch* b) {
     B_CUDA(ct::launch_batch_metrics_dev(d, &b->epoch_dev[i].batch_index, ss));
   }
   B_CUDA(join_side(b));
+  B_CUDA(batch_mark(b, CT_PHASE_UPDATE));
   return cudaSuccess;
 }
 
@@ -1544,9 +1586,6 @@ int ct_batch_create(ct_ctx* ctx, ct_scn* const* scenarios, int64_t count, int gr
     if (s->ctx != ctx) return fail(CT_ERR_INVALID_ARGUMENT, "scenario %lld belongs to another context", (long long)i);
     if (s->algo.batch_size != 0)
       return fail(CT_ERR_NOT_SUPPORTED, "scenario %lld: batches need batch_size 0 (one update per epoch)",
-                  (long long)i);
-    if (precision != CT_PREC_FP32 && !s->d.umma)
-      return fail(CT_ERR_NOT_SUPPORTED, "scenario %lld: tensor-core precision needs num_states divisible by 4",
                   (long long)i);
     for (int64_t j = 0; j < i; ++j)
       if (scenarios[j] == s) return fail(CT_ERR_INVALID_ARGUMENT, "scenario %lld appears twice", (long long)i);
@@ -1665,7 +1704,7 @@ int ct_batch_run_epoch(ct_batch* b, int64_t* batch_indices) {
   // pageable source: the copy is staged before the call returns, so `ep` may go out of scope
   CT_CUDA(cudaMemcpyAsync(b->epoch_dev, ep.data(), sizeof(EpochDev) * n, cudaMemcpyHostToDevice, st),
           "batch epoch scalars");
-  if (b->exec) {
+  if (b->exec && !b->profiling) {
     CT_CUDA(cudaGraphLaunch(b->exec, st), "cudaGraphLaunch");
   } else {
     CT_CUDA(batch_enqueue_epoch(b), "batch epoch");
@@ -1685,6 +1724,31 @@ int ct_batch_sync(ct_batch* b) {
     int rc = ct_sync(s);
     if (rc) return rc;
   }
+  return CT_OK;
+}
+
+int ct_batch_set_profiling(ct_batch* b, int enable) {
+  if (!b) return fail(CT_ERR_INVALID_ARGUMENT, "batch is NULL");
+  b->profiling = enable != 0;
+  for (double& m : b->phase_ms) m = 0.0;
+  return CT_OK;
+}
+
+int ct_batch_read_profile(ct_batch* b, double* ms) {
+  if (!b || !ms) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  CT_CUDA(cudaSetDevice(b->ctx->device), "cudaSetDevice");
+  CT_CUDA(cudaStreamSynchronize(b->ctx->stream), "cudaStreamSynchronize");
+  for (auto& pe : b->pending) {
+    float t = 0.0f;
+    CT_CUDA(cudaEventElapsedTime(&t, pe.start, pe.stop), "cudaEventElapsedTime");
+    b->phase_ms[pe.phase] += t;
+    cudaEventDestroy(pe.start);
+    cudaEventDestroy(pe.stop);
+  }
+  b->pending.clear();
+  if (b->open_event) cudaEventDestroy(b->open_event);
+  b->open_event = nullptr;
+  for (int i = 0; i < CT_PHASE_COUNT; ++i) ms[i] = b->phase_ms[i];
   return CT_OK;
 }
 

@@ -181,7 +181,8 @@ int ct_run_epoch_plain(ct_scn* scn, int64_t* batch_index, const int32_t* beat_or
  * reference derivations, then every member's update. The epoch is captured once as a CUDA
  * graph and replayed (re-captured when a member's algorithm or adjoint ring changes).
  * Members need batch_size 0 (one update per epoch, the reference default) and the same
- * context; their beats run in index order. Results equal ct_run_epoch with beat_order
+ * context; their beats run in index order. With a tensor-core precision, members whose
+ * num_states is not a multiple of 4 use the FP32 products. Results equal ct_run_epoch with beat_order
  * 0..B-1 within the tolerances of the measurement products. The members stay usable on
  * their own; a batch must be destroyed before its members. */
 typedef struct ct_batch ct_batch;
@@ -195,6 +196,12 @@ int ct_batch_run_epoch(ct_batch* batch, int64_t* batch_indices);
 int ct_batch_sync(ct_batch* batch);
 /* Kernel nodes in the captured epoch graph, and whether the graph is used (0: eager launches). */
 int ct_batch_info(ct_batch* batch, int64_t* graph_kernels, int* uses_graph);
+/* Per-phase device time of batched epochs: while enabled, epochs run as eager launches (not the
+ * graph) with CUDA events around each phase; ct_batch_read_profile waits for the batch and writes
+ * CT_PHASE_COUNT totals in ms since enabling (FORWARD: memsets + forward launches; MEASURE: the
+ * members' products, reference derivations and step metrics; DERIVE: adjoint launches; UPDATE). */
+int ct_batch_set_profiling(ct_batch* batch, int enable);
+int ct_batch_read_profile(ct_batch* batch, double* ms);
 
 /* Forward of every beat with the current parameters (no noise); writes the predicted
  * measurements [B,T,M] and, if non-NULL, the states [T,S] of the last beat. Synchronous. */
