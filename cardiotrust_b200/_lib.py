@@ -80,6 +80,7 @@ EXPORTED = [
     "ct_batch_run_epoch",
     "ct_batch_sync",
     "ct_batch_info",
+    "ct_batch_autotune",
     "ct_batch_set_profiling",
     "ct_batch_read_profile",
     "ct_simulate",
@@ -172,6 +173,8 @@ def load(path: pathlib.Path = LIB_PATH) -> ctypes.CDLL:
     lib.ct_batch_sync.argtypes = [vp]
     lib.ct_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int)]
     lib.ct_batch_set_profiling.argtypes = [vp, ctypes.c_int]
+    lib.ct_batch_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
     lib.ct_batch_read_profile.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.ct_simulate.argtypes = [vp, _fp, _fp]
     lib.ct_set_algorithm.argtypes = [vp, ctypes.POINTER(CtAlgorithm)]

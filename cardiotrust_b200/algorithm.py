@@ -344,6 +344,13 @@ class EpochBatch:
         check(lib().ct_batch_info(self._h, ctypes.byref(k), ctypes.byref(g)))
         return {"graph_kernels": int(k.value), "uses_graph": bool(g.value)}
 
+    def autotune(self) -> dict:
+        """Time candidate schedules on real epochs (they train) and keep the fastest; see ct_batch_autotune."""
+        k, o, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(lib().ct_batch_autotune(self._h, self.batch_indices.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                      ctypes.byref(k), ctypes.byref(o), ctypes.byref(ms)))
+        return {"ckpt_steps": k.value, "tile_order": o.value, "epoch_ms": ms.value}
+
     def set_profiling(self, enable: bool) -> None:
         """Per-phase CUDA-event timing of batched epochs (eager launches while enabled)."""
         check(lib().ct_batch_set_profiling(self._h, int(enable)))

@@ -1273,6 +1273,10 @@ struct ct_batch {
   std::vector<int> captured_ring;
   std::vector<uint64_t> captured_gen;
   int64_t graph_kernels = 0;
+  // tuned choices (ct_batch_autotune): adjoint checkpoint interval, tile order
+  int ckpt_k = kBatchCkptSteps;
+  int tile_order = 0;
+  int captured_k = 0;
   // optional per-phase timing (eager launches, CUDA events on the context stream)
   bool profiling = false;
   cudaEvent_t open_event = nullptr;
@@ -1440,7 +1444,7 @@ cudaError_t batch_enqueue_epoch(ct_batch* b) {
       al.tiles = fb.tiles;
       al.ntiles = fb.ntiles;
       al.Tmax = fb.Tmax;
-      al.ckpt_steps = kBatchCkptSteps;
+      al.ckpt_steps = b->ckpt_k;
       al.status = d0.status;
       al.barrier = d0.barrier;
       B_CUDA(batch_mark(b, CT_PHASE_MEASURE));
@@ -1485,13 +1489,14 @@ int batch_prepare(ct_batch* b) {
     ct_scn* s = b->scns[i];
     if (b->grad_mode == CT_GRAD_ADJOINT) {
       const int before = s->d.adj_ring;
-      int rc = prepare_adjoint(s, kBatchCkptSteps);
+      int rc = prepare_adjoint(s, b->ckpt_k);
       if (rc) return rc;
       if (s->d.adj_ring != before) stale = true;
     }
     if (b->captured_ring.size() == n && b->captured_ring[i] != s->d.adj_ring) stale = true;
     if (b->captured_gen.size() == n && b->captured_gen[i] != s->config_gen) stale = true;
   }
+  if (b->captured_k != b->ckpt_k) stale = true;
   if (!stale && b->captured_ring.size() == n) return CT_OK;
   // descriptors
   std::vector<ct::FwdArgs> fa(n);
@@ -1559,12 +1564,63 @@ int batch_prepare(ct_batch* b) {
       b->use_graph = false;
     }
   }
+  b->captured_k = b->ckpt_k;
   b->captured_ring.assign(n, 0);
   b->captured_gen.assign(n, 0);
   for (size_t i = 0; i < n; ++i) {
     b->captured_ring[i] = b->scns[i]->d.adj_ring;
     b->captured_gen[i] = b->scns[i]->config_gen;
   }
+  return CT_OK;
+}
+
+// Tile lists per beat index. Order 0: scenarios by decreasing beat length, each scenario's tiles
+// together, so that at any step the live tiles form a prefix of the list, which the round-robin
+// tile -> CTA assignment (CTA c takes tiles c, c + G, ...) spreads evenly. Order 1: the same list
+// folded back and forth over the adjoint grid (chunk k of G tiles reversed when k is odd), so that
+// no CTA always gets the first tile of a chunk. Order 2: scenarios by decreasing beat length, their
+// tiles interleaved one at a time.
+int batch_build_tiles(ct_batch* b, bool upload) {
+  const size_t n = b->scns.size();
+  std::vector<size_t> order(n);
+  for (size_t i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return b->scns[x]->d.T > b->scns[y]->d.T; });
+  b->beat_tiles.assign((size_t)b->nbeats_max, {});
+  b->beat_tmax.assign((size_t)b->nbeats_max, 0);
+  for (int beat = 0; beat < b->nbeats_max; ++beat) {
+    std::vector<int2>& tl = b->beat_tiles[(size_t)beat];
+    if (b->tile_order == 2) {
+      for (int t = 0;; ++t) {
+        bool any = false;
+        for (size_t i : order) {
+          DeviceScenario& d = b->scns[i]->d;
+          if (beat >= d.B || t >= b->ntiles[i]) continue;
+          tl.push_back(make_int2((int)i, t * ct::kFwdTileVoxels));
+          any = true;
+        }
+        if (!any) break;
+      }
+    } else {
+      for (size_t i : order) {
+        DeviceScenario& d = b->scns[i]->d;
+        if (beat >= d.B) continue;
+        for (int t = 0; t < b->ntiles[i]; ++t) tl.push_back(make_int2((int)i, t * ct::kFwdTileVoxels));
+      }
+      if (b->tile_order == 1 && b->adj_grid > 0) {
+        const size_t G = (size_t)b->adj_grid;
+        for (size_t k = 1; k * G < tl.size(); k += 2)
+          std::reverse(tl.begin() + (ptrdiff_t)(k * G), tl.begin() + (ptrdiff_t)std::min(tl.size(), (k + 1) * G));
+      }
+    }
+    for (const int2& t : tl)
+      b->beat_tmax[(size_t)beat] = std::max<int>(b->beat_tmax[(size_t)beat], (int)b->scns[(size_t)t.x]->d.T);
+  }
+  if (upload)
+    for (int beat = 0; beat < b->nbeats_max; ++beat) {
+      const auto& tl = b->beat_tiles[(size_t)beat];
+      CT_CUDA(cudaMemcpy(b->beat_tiles_dev[(size_t)beat], tl.data(), sizeof(int2) * tl.size(), cudaMemcpyHostToDevice),
+              "batch tiles");
+    }
   return CT_OK;
 }
 
@@ -1598,29 +1654,15 @@ int ct_batch_create(ct_ctx* ctx, ct_scn* const* scenarios, int64_t count, int gr
   b->scns.assign(scenarios, scenarios + count);
   const size_t n = b->scns.size();
   int rc = CT_OK;
-  // tiles: scenarios by decreasing beat length, so that at any step the live tiles form a prefix of the
-  // list, which the round-robin tile -> CTA assignment spreads evenly
-  std::vector<size_t> order(n);
-  for (size_t i = 0; i < n; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return b->scns[x]->d.T > b->scns[y]->d.T; });
   b->ntiles.resize(n);
   for (size_t i = 0; i < n; ++i) {
     DeviceScenario& d = b->scns[i]->d;
     b->ntiles[i] = (int)((d.V + ct::kFwdTileVoxels - 1) / ct::kFwdTileVoxels);
     b->nbeats_max = std::max<int>(b->nbeats_max, (int)d.B);
   }
-  b->beat_tiles.resize((size_t)b->nbeats_max);
-  b->beat_tmax.assign((size_t)b->nbeats_max, 0);
-  for (int beat = 0; beat < b->nbeats_max; ++beat)
-    for (size_t i : order) {
-      DeviceScenario& d = b->scns[i]->d;
-      if (beat >= d.B) continue;
-      b->beat_tmax[(size_t)beat] = std::max<int>(b->beat_tmax[(size_t)beat], (int)d.T);
-      for (int t = 0; t < b->ntiles[i]; ++t)
-        b->beat_tiles[(size_t)beat].push_back(make_int2((int)i, t * ct::kFwdTileVoxels));
-    }
   b->fwd_grid = ct::forward_batch_capacity(ctx->device);
   b->adj_grid = ct::adjoint_capacity(ctx->device);
+  batch_build_tiles(b, false);
   void* p = nullptr;
   rc = batch_alloc(b, &p, sizeof(ct::FwdArgs) * n);
   b->fwd_dev = static_cast<ct::FwdArgs*>(p);
@@ -1715,6 +1757,75 @@ int ct_batch_run_epoch(ct_batch* b, int64_t* batch_indices) {
     batch_indices[i] += 1;
     if (!s->algo.freeze_delays) note_delay_update(s, st);
   }
+  return CT_OK;
+}
+
+int ct_batch_autotune(ct_batch* b, int64_t* batch_indices, int* ckpt_k, int* tile_order, double* best_ms) {
+  if (!b || !batch_indices) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  CT_CUDA(cudaSetDevice(b->ctx->device), "cudaSetDevice");
+  cudaStream_t st = b->ctx->stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CT_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
+  CT_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
+  const bool was_profiling = b->profiling;
+  b->profiling = false;
+  auto trial = [&](int k, int order, double* ms) -> int {
+    b->ckpt_k = k;
+    b->tile_order = order;
+    int rc = batch_build_tiles(b, true);
+    if (rc) return rc;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->captured_ring.clear();
+    rc = batch_prepare(b);  // re-layout for k, capture
+    if (rc) return rc;
+    CT_CUDA(cudaStreamSynchronize(st), "autotune");
+    CT_CUDA(cudaEventRecord(e0, st), "cudaEventRecord");
+    rc = ct_batch_run_epoch(b, batch_indices);
+    if (rc) return rc;
+    CT_CUDA(cudaEventRecord(e1, st), "cudaEventRecord");
+    rc = ct_batch_sync(b);
+    if (rc) return rc;
+    float t = 0.0f;
+    CT_CUDA(cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime");
+    *ms = t;
+    return CT_OK;
+  };
+  int best_k = b->ckpt_k, best_o = b->tile_order;
+  double best = 1e300;
+  int rc = CT_OK;
+  const int ks[3] = {32, 64, 128};
+  for (int k : ks) {
+    double ms = 0.0;
+    if (b->grad_mode != CT_GRAD_ADJOINT && k != kBatchCkptSteps) continue;  // the interval only matters for adjoint
+    rc = trial(k, 0, &ms);
+    if (rc) break;
+    if (ms < best) best = ms, best_k = k, best_o = 0;
+  }
+  for (int o = 1; o <= 2 && !rc; ++o) {
+    double ms = 0.0;
+    rc = trial(best_k, o, &ms);
+    if (rc) break;
+    if (ms < best) best = ms, best_o = o;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->profiling = was_profiling;
+  if (rc) return rc;
+  b->ckpt_k = best_k;
+  b->tile_order = best_o;
+  rc = batch_build_tiles(b, true);
+  if (rc) return rc;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->captured_ring.clear();
+  if (ckpt_k) *ckpt_k = best_k;
+  if (tile_order) *tile_order = best_o;
+  if (best_ms) *best_ms = best;
   return CT_OK;
 }
 

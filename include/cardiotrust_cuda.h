@@ -192,6 +192,13 @@ int ct_batch_destroy(ct_batch* batch);
 /* One epoch of every member, enqueued on the context stream (asynchronous).
  * batch_indices: in/out batch-wise metric cursor per member (as ct_run_epoch's batch_index). */
 int ct_batch_run_epoch(ct_batch* batch, int64_t* batch_indices);
+/* Autotuner: runs real epochs of the batch (each one trains and advances batch_indices like
+ * ct_batch_run_epoch) under candidate schedules and keeps the fastest: the adjoint checkpoint
+ * interval (32, 64, 128 steps; memory against recompute granularity) and the order of the tile
+ * lists (by beat length; folded over the grid; interleaved across members), which sets how the
+ * tiles of members of different sizes spread over the CTAs. Up to five epochs; synchronous.
+ * Writes the choice and its epoch time (ms) to the non-NULL outputs. */
+int ct_batch_autotune(ct_batch* batch, int64_t* batch_indices, int* ckpt_k, int* tile_order, double* best_ms);
 /* Waits for the batch and reports any device-side failure of a member. */
 int ct_batch_sync(ct_batch* batch);
 /* Kernel nodes in the captured epoch graph, and whether the graph is used (0: eager launches). */

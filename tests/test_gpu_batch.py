@@ -48,7 +48,7 @@ def members(oracle_mod):
 
 
 def _engines(alg, ctx, members, algo):
-    return [alg.EpochEngine.from_scenario(ctx, m, num_batch_slots=4, algorithm=algo) for m in members]
+    return [alg.EpochEngine.from_scenario(ctx, m, num_batch_slots=8, algorithm=algo) for m in members]
 
 
 @pytest.mark.parametrize("mode", ["reference", "adjoint"])
@@ -126,6 +126,30 @@ def test_batch_recaptures_after_algorithm_change(alg, ctx, members):
         e.run_epoch(1, beat_order=np.arange(m.num_beats))
     for b, e in zip(batched, single):
         assert rel_err(b.read("gains"), e.read("gains")) < 1e-6
+    batch.close()
+    for e in batched + single:
+        e.close()
+
+
+def test_batch_autotune_trains_like_single_runs(alg, ctx, members):
+    """The autotuner's trial epochs are real epochs: after it, every member has trained exactly as many
+    epochs as its one-at-a-time twin (schedules change the order of nothing but independent work)."""
+    algo = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
+    batched = _engines(alg, ctx, members, algo)
+    single = _engines(alg, ctx, members, algo)
+    batch = alg.EpochBatch(ctx, batched, grad_mode=alg.GradMode.Adjoint)
+    choice = batch.autotune()
+    assert choice["ckpt_steps"] in (32, 64, 128) and choice["tile_order"] in (0, 1, 2) and choice["epoch_ms"] > 0
+    epochs = int(batch.batch_indices[0])
+    assert epochs == 5 and all(int(i) == epochs for i in batch.batch_indices)
+    batch.run_epoch()
+    for m, e in zip(members, single):
+        for ep in range(epochs + 1):
+            e.run_epoch(ep, beat_order=np.arange(m.num_beats), grad_mode=alg.GradMode.Adjoint)
+    for b, e in zip(batched, single):
+        assert rel_err(b.read("gains"), e.read("gains")) < 1e-5
+        assert rel_err(b.read("coefs"), e.read("coefs")) < 1e-5
+        np.testing.assert_array_equal(b.read("delays"), e.read("delays"))
     batch.close()
     for e in batched + single:
         e.close()
