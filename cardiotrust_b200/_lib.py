@@ -22,6 +22,8 @@ CT_ERR_TIMEOUT = -4
 CT_ERR_INVALID_INDEX = -5
 CT_ERR_NOT_SUPPORTED = -6
 CT_ERR_BATCH_INDEX = -7
+CT_ERR_NO_MAXIMUM = -8
+CT_THRESHOLDS = 101
 
 CT_OPT_SGD, CT_OPT_ADAM = 0, 1
 CT_AP_SIMPLE, CT_AP_TEXTBOOK = 0, 1
@@ -61,6 +63,23 @@ FIELDS = {
     "loss_batch": (43, np.float32, lambda S, V, M, T, B, NB: (NB,)),
     "loss_mse_batch": (44, np.float32, lambda S, V, M, T, B, NB: (NB,)),
     "loss_maximum_regularization_batch": (45, np.float32, lambda S, V, M, T, B, NB: (NB,)),
+    "system_states_magnitude": (50, np.float32, lambda S, V, M, T, B, NB: (T, V)),
+    "system_states_theta": (51, np.float32, lambda S, V, M, T, B, NB: (T, V)),
+    "system_states_phi": (52, np.float32, lambda S, V, M, T, B, NB: (T, V)),
+    "system_states_magnitude_max": (53, np.float32, lambda S, V, M, T, B, NB: (V,)),
+    "system_states_theta_max": (54, np.float32, lambda S, V, M, T, B, NB: (V,)),
+    "system_states_phi_max": (55, np.float32, lambda S, V, M, T, B, NB: (V,)),
+    "activation_times": (56, np.float32, lambda S, V, M, T, B, NB: (V,)),
+}
+
+# Snapshot fields: (ct_field, dtype, per-snapshot shape); the leading snapshot count comes from
+# ct_field_size.
+SNAPSHOT_FIELDS = {
+    "gains": (60, np.float32, lambda S, V, M, T, B: (S, 78)),
+    "coefs": (61, np.float32, lambda S, V, M, T, B: (V, 26)),
+    "delays": (62, np.int32, lambda S, V, M, T, B: (V, 26)),
+    "system_states": (63, np.float32, lambda S, V, M, T, B: (T, S)),
+    "measurements": (64, np.float32, lambda S, V, M, T, B: (B, T, M)),
 }
 
 EXPORTED = [
@@ -95,6 +114,10 @@ EXPORTED = [
     "ct_set_profiling",
     "ct_read_profile",
     "ct_predict_measurements_noalloc",
+    "ct_run_model_based",
+    "ct_batch_run_model_based",
+    "ct_calculate_plotting_arrays",
+    "ct_calculate_final",
 ]
 
 PHASES = ["forward", "measure", "map_residuals", "derive", "step_metrics", "update"]
@@ -136,6 +159,41 @@ class CtScenarioDesc(ctypes.Structure):
         ("control_matrix", _fp),
         ("control_function", _fp),
         ("measurements", _fp),
+    ]
+
+
+class CtRunConfig(ctypes.Structure):
+    _fields_ = [
+        ("epochs", ctypes.c_int64),
+        ("learning_rate_reduction_interval", ctypes.c_int64),
+        ("learning_rate_reduction_factor", ctypes.c_float),
+        ("grad_mode", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("snapshots_interval", ctypes.c_int64),
+    ]
+
+
+class CtRunSummary(ctypes.Structure):
+    _fields_ = [
+        ("epochs_run", ctypes.c_int64),
+        ("snapshots", ctypes.c_int64),
+        ("loss", ctypes.c_float),
+        ("loss_mse", ctypes.c_float),
+        ("loss_maximum_regularization", ctypes.c_float),
+    ]
+
+
+class CtFinalMetrics(ctypes.Structure):
+    _fields_ = [
+        ("dice_score_over_threshold", ctypes.c_float * CT_THRESHOLDS),
+        ("iou_over_threshold", ctypes.c_float * CT_THRESHOLDS),
+        ("precision_over_threshold", ctypes.c_float * CT_THRESHOLDS),
+        ("recall_over_threshold", ctypes.c_float * CT_THRESHOLDS),
+        ("threshold", ctypes.c_float),
+        ("dice", ctypes.c_float),
+        ("iou", ctypes.c_float),
+        ("recall", ctypes.c_float),
+        ("precision", ctypes.c_float),
     ]
 
 
@@ -189,6 +247,13 @@ def load(path: pathlib.Path = LIB_PATH) -> ctypes.CDLL:
     lib.ct_read_profile.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
     lib.ct_predict_measurements_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int64, ctypes.c_int64,
                                                     ctypes.c_int64, vp]
+    lib.ct_run_model_based.argtypes = [vp, ctypes.POINTER(CtRunConfig), _ip, ctypes.POINTER(ctypes.c_int64), _fp,
+                                       ctypes.POINTER(CtRunSummary)]
+    lib.ct_batch_run_model_based.argtypes = [vp, ctypes.POINTER(CtRunConfig), ctypes.POINTER(ctypes.c_int64), _fp,
+                                             ctypes.POINTER(CtRunSummary)]
+    lib.ct_calculate_plotting_arrays.argtypes = [vp, ctypes.c_float]
+    lib.ct_calculate_final.argtypes = [vp, _ip, _ip, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                       ctypes.POINTER(CtFinalMetrics)]
     for name in EXPORTED:
         getattr(lib, name)  # AttributeError if a declared symbol is not exported
     return lib

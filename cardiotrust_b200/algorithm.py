@@ -55,7 +55,10 @@ class Algorithm:
     optimizer: Optimizer = Optimizer.Sgd
     epochs: int = 10
     batch_size: int = 0
+    snapshots_interval: int = 0
     learning_rate: float = 200.0
+    learning_rate_reduction_factor: float = 0.0
+    learning_rate_reduction_interval: int = 0
     mse_strength: float = 1.0
     slow_down_stregth: float = 0.0  # read by nothing on the epoch path (update.rs:163-167)
     maximum_regularization_strength: float = 1.0
@@ -65,6 +68,17 @@ class Algorithm:
     freeze_gains: bool = False
     freeze_delays: bool = True
     ap_derivative: APDerivative = APDerivative.Textbook
+
+    def run_config(self, grad_mode=None, precision=None) -> _lib.CtRunConfig:
+        """The epoch-loop settings of run_model_based (scenario.rs:725-795)."""
+        c = _lib.CtRunConfig()
+        c.epochs = int(self.epochs)
+        c.learning_rate_reduction_interval = int(self.learning_rate_reduction_interval)
+        c.learning_rate_reduction_factor = float(self.learning_rate_reduction_factor)
+        c.grad_mode = int(GradMode.Reference if grad_mode is None else grad_mode)
+        c.precision = int(Precision.Fp32 if precision is None else precision)
+        c.snapshots_interval = int(self.snapshots_interval)
+        return c
 
     def to_ct(self) -> _lib.CtAlgorithm:
         a = _lib.CtAlgorithm()
@@ -240,6 +254,55 @@ class EpochEngine:
         check(lib().ct_read_profile(self._h, ms, cnt))
         return {p: (ms[i], cnt[i]) for i, p in enumerate(_lib.PHASES)}
 
+    def run_model_based(self, batch_index: int = 0, beat_orders=None, grad_mode=GradMode.Reference,
+                        precision=Precision.Fp32, algorithm: Optional[Algorithm] = None):
+        """The reference's epoch loop (scenario.rs:725-795) with this engine's algorithm settings:
+        learning-rate schedule, per-epoch summary, snapshots, early stop on a non-normal loss, final
+        average delays. Returns (summary dict, [epochs_run, 3] per-epoch losses, batch index)."""
+        a = algorithm or self.algorithm
+        cfg = a.run_config(grad_mode, precision)
+        losses = np.zeros((max(int(a.epochs), 1), 3), dtype=np.float32)
+        order = None
+        if beat_orders is not None:
+            order = _i32(beat_orders)
+            if order.shape != (int(a.epochs), self.dims["B"]):
+                raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, f"beat_orders must be [{a.epochs}, {self.dims['B']}]")
+        bi = ctypes.c_int64(int(batch_index))
+        summ = _lib.CtRunSummary()
+        check(lib().ct_run_model_based(self._h, ctypes.byref(cfg), None if order is None else iptr(order),
+                                       ctypes.byref(bi), fptr(losses), ctypes.byref(summ)))
+        out = {f: getattr(summ, f) for f, _ in _lib.CtRunSummary._fields_}
+        return out, losses[: summ.epochs_run].copy(), bi.value
+
+    def calculate_plotting_arrays(self, sample_rate_hz: float) -> None:
+        """Spherical arrays, their maxima and activation times of the last beat's states
+        (scenario.rs:636-690, estimation side); read them as ``system_states_*`` / ``activation_times``."""
+        check(lib().ct_calculate_plotting_arrays(self._h, float(sample_rate_hz)))
+
+    def calculate_final(self, ground_truth_types, voxel_numbers) -> "FinalMetrics":
+        """metrics::calculate_final (metrics.rs:226-447) on the last beat's states, and the summary at
+        the Dice-optimal threshold (scenario.rs:601-617)."""
+        t = _i32(ground_truth_types)
+        n = _i32(voxel_numbers)
+        if t.shape != n.shape or t.ndim != 3:
+            raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, "ground truth types and voxel numbers must be the same 3-d grid")
+        m = _lib.CtFinalMetrics()
+        check(lib().ct_calculate_final(self._h, iptr(t), iptr(n), *t.shape, ctypes.byref(m)))
+        return FinalMetrics.from_ct(m)
+
+    def read_snapshots(self, name: str) -> np.ndarray:
+        """Snapshots of the last run_model_based call: gains, coefs, delays, system_states or
+        measurements, with a leading snapshot axis (Snapshots, results.rs:179-248)."""
+        code, dtype, shape = _lib.SNAPSHOT_FIELDS[name]
+        D = self.dims
+        per = shape(D["S"], D["V"], D["M"], D["T"], D["B"])
+        nbytes = ctypes.c_size_t()
+        check(lib().ct_field_size(self._h, code, ctypes.byref(nbytes)))
+        n = nbytes.value // (int(np.prod(per)) * np.dtype(dtype).itemsize)
+        out = np.empty((n, *per), dtype=dtype)
+        check(lib().ct_read_field(self._h, code, out.ctypes.data_as(ctypes.c_void_p), out.nbytes))
+        return out
+
     # -- fields
     def read(self, name: str) -> np.ndarray:
         code, dtype, shape = _lib.FIELDS[name]
@@ -351,6 +414,21 @@ class EpochBatch:
                                       ctypes.byref(k), ctypes.byref(o), ctypes.byref(ms)))
         return {"ckpt_steps": k.value, "tile_order": o.value, "epoch_ms": ms.value}
 
+    def run_model_based(self, algorithm: Algorithm, grad_mode=GradMode.Reference, precision=Precision.Fp32):
+        """The reference's epoch loop over every member (ct_batch_run_model_based): each member follows
+        its own learning rate through ``algorithm``'s schedule and stops on its own non-normal loss.
+        ``grad_mode`` / ``precision`` must be the batch's. Returns (per-member summary dicts,
+        [members, epochs, 3] losses; rows past a member's last epoch are NaN)."""
+        cfg = algorithm.run_config(grad_mode, precision)
+        n = len(self._engines)
+        losses = np.full((n, max(int(algorithm.epochs), 1), 3), np.nan, dtype=np.float32)
+        summ = (_lib.CtRunSummary * n)()
+        check(lib().ct_batch_run_model_based(self._h, ctypes.byref(cfg),
+                                             self.batch_indices.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                             fptr(losses), summ))
+        out = [{f: getattr(summ[i], f) for f, _ in _lib.CtRunSummary._fields_} for i in range(n)]
+        return out, losses[:, : int(algorithm.epochs)]
+
     def set_profiling(self, enable: bool) -> None:
         """Per-phase CUDA-event timing of batched epochs (eager launches while enabled)."""
         check(lib().ct_batch_set_profiling(self._h, int(enable)))
@@ -426,3 +504,73 @@ def run_epoch(results: Results, batch_index: BatchIndex, data: Data, config: Alg
         results._data_id = id(data)
     eng.set_algorithm(config)
     batch_index.value = eng.run_epoch(batch_index.value, beat_order=beat_order)
+
+
+@dataclasses.dataclass
+class FinalMetrics:
+    """Metrics::*_over_threshold (metrics.rs:20-37) and the Summary fields at the Dice-optimal threshold."""
+
+    dice_score_over_threshold: np.ndarray
+    iou_over_threshold: np.ndarray
+    precision_over_threshold: np.ndarray
+    recall_over_threshold: np.ndarray
+    threshold: float
+    dice: float
+    iou: float
+    recall: float
+    precision: float
+
+    @classmethod
+    def from_ct(cls, m: _lib.CtFinalMetrics) -> "FinalMetrics":
+        arr = lambda f: np.ctypeslib.as_array(getattr(m, f)).astype(np.float32).copy()  # noqa: E731
+        return cls(arr("dice_score_over_threshold"), arr("iou_over_threshold"), arr("precision_over_threshold"),
+                   arr("recall_over_threshold"), float(m.threshold), float(m.dice), float(m.iou), float(m.recall),
+                   float(m.precision))
+
+
+@dataclasses.dataclass
+class Summary:
+    """``Summary`` (summary.rs:25-42)."""
+
+    loss: float = 0.0
+    loss_mse: float = 0.0
+    loss_maximum_regularization: float = 0.0
+    dice: float = 0.0
+    iou: float = 0.0
+    precision: float = 0.0
+    recall: float = 0.0
+    threshold: float = 0.0
+
+
+def run_model_based(results: Results, data: Data, config: Algorithm, beat_orders=None,
+                    grad_mode=GradMode.Reference, precision=Precision.Fp32) -> Summary:
+    """``run_model_based`` (scenario.rs:725-795) on the GPU: ``config.epochs`` epochs under the
+    learning-rate schedule, snapshots every ``config.snapshots_interval`` epochs (read them with
+    ``results.engine.read_snapshots``), early stop when the loss is not normal, then the average
+    delays of the final parameters. The returned Summary carries the loss fields."""
+    eng = results.engine
+    if results._data_id != id(data):
+        eng.write("measurements_actual", data.measurements)
+        results._data_id = id(data)
+    eng.set_algorithm(config)
+    summ, _, bi = eng.run_model_based(0, beat_orders=beat_orders, grad_mode=grad_mode, precision=precision,
+                                      algorithm=config)
+    results.batch_index = bi
+    results.epochs_run = summ["epochs_run"]
+    return Summary(loss=summ["loss"], loss_mse=summ["loss_mse"],
+                   loss_maximum_regularization=summ["loss_maximum_regularization"])
+
+
+def calculate_plotting_arrays(results: Results, sample_rate_hz: float) -> None:
+    """Estimation side of ``calculate_plotting_arrays`` (scenario.rs:636-690)."""
+    results.engine.calculate_plotting_arrays(sample_rate_hz)
+
+
+def calculate_final(results: Results, ground_truth_types, voxel_numbers, summary: Optional[Summary] = None):
+    """``metrics::calculate_final`` (metrics.rs:226-242) plus the Dice-optimal summary fields
+    (scenario.rs:601-617), filled into ``summary`` when given."""
+    m = results.engine.calculate_final(ground_truth_types, voxel_numbers)
+    if summary is not None:
+        summary.threshold, summary.dice, summary.iou = m.threshold, m.dice, m.iou
+        summary.recall, summary.precision = m.recall, m.precision
+    return m

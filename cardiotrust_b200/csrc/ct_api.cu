@@ -69,6 +69,17 @@ struct ct_scn {
   int64_t phase_launches[CT_PHASE_COUNT] = {};
   std::vector<PhaseEvents> pending;
   std::vector<cudaEvent_t> event_pool;
+  // post-run pass (ct_calculate_plotting_arrays / ct_calculate_final), allocated on first use
+  ct::PostBuffers post{};
+  ct::PostPlan post_plan{};
+  bool post_arrays = false;  // CT_FIELD_STATES_* / CT_FIELD_ACTIVATION_TIMES hold results
+  // snapshots of the last ct_run_model_based call: snap_n stored slots of snap_cap allocated
+  int64_t snap_n = 0, snap_cap = 0;
+  float* snap_gains = nullptr;
+  float* snap_coefs = nullptr;
+  int32_t* snap_delays = nullptr;
+  float* snap_X = nullptr;
+  float* snap_Y = nullptr;
 };
 
 namespace {
@@ -604,6 +615,18 @@ int field_bytes(const ct_scn* s, int field, size_t* nbytes) {
     case CT_FIELD_LOSS_BATCH:
     case CT_FIELD_LOSS_MSE_BATCH:
     case CT_FIELD_LOSS_MAXIMUM_REGULARIZATION_BATCH: *nbytes = f * d.NB; return CT_OK;
+    case CT_FIELD_STATES_MAGNITUDE:
+    case CT_FIELD_STATES_THETA:
+    case CT_FIELD_STATES_PHI: *nbytes = f * d.T * d.V; return CT_OK;
+    case CT_FIELD_STATES_MAGNITUDE_MAX:
+    case CT_FIELD_STATES_THETA_MAX:
+    case CT_FIELD_STATES_PHI_MAX:
+    case CT_FIELD_ACTIVATION_TIMES: *nbytes = f * d.V; return CT_OK;
+    case CT_FIELD_SNAPSHOT_GAINS: *nbytes = f * s->snap_n * d.S * kGainCols; return CT_OK;
+    case CT_FIELD_SNAPSHOT_COEFS: *nbytes = f * s->snap_n * d.V * kOffsets; return CT_OK;
+    case CT_FIELD_SNAPSHOT_DELAYS: *nbytes = sizeof(int32_t) * s->snap_n * d.V * kOffsets; return CT_OK;
+    case CT_FIELD_SNAPSHOT_SYSTEM_STATES: *nbytes = f * s->snap_n * d.T * d.S; return CT_OK;
+    case CT_FIELD_SNAPSHOT_MEASUREMENTS: *nbytes = f * s->snap_n * d.B * d.T * d.M; return CT_OK;
     default: return fail(CT_ERR_INVALID_ARGUMENT, "unknown field %d", field);
   }
 }
@@ -667,6 +690,7 @@ const char* ct_status_string(int status) {
     case CT_ERR_INVALID_INDEX: return "output_state_indices lack the voxel/neighbour structure";
     case CT_ERR_NOT_SUPPORTED: return "not supported";
     case CT_ERR_BATCH_INDEX: return "batch index outside the metric arrays";
+    case CT_ERR_NO_MAXIMUM: return "a voxel's magnitude is NaN at every step";
     default: return "unknown status";
   }
 }
@@ -1120,6 +1144,49 @@ int ct_read_field(ct_scn* scn, int field, void* dst, size_t nbytes) {
     case CT_FIELD_LOSS_BATCH: return copy_down(scn, dst, d.loss_b, nbytes);
     case CT_FIELD_LOSS_MSE_BATCH: return copy_down(scn, dst, d.loss_mse_b, nbytes);
     case CT_FIELD_LOSS_MAXIMUM_REGULARIZATION_BATCH: return copy_down(scn, dst, d.loss_mr_b, nbytes);
+    case CT_FIELD_STATES_MAGNITUDE:
+    case CT_FIELD_STATES_THETA:
+    case CT_FIELD_STATES_PHI:
+    case CT_FIELD_STATES_MAGNITUDE_MAX:
+    case CT_FIELD_STATES_THETA_MAX:
+    case CT_FIELD_STATES_PHI_MAX:
+    case CT_FIELD_ACTIVATION_TIMES: {
+      if (!scn->post_arrays) return fail(CT_ERR_INVALID_ARGUMENT, "field %d: call ct_calculate_plotting_arrays first", field);
+      const ct::PostBuffers& b = scn->post;
+      const float* src = field == CT_FIELD_STATES_MAGNITUDE     ? b.mag
+                         : field == CT_FIELD_STATES_THETA       ? b.theta
+                         : field == CT_FIELD_STATES_PHI         ? b.phi
+                         : field == CT_FIELD_STATES_MAGNITUDE_MAX ? b.mag_max
+                         : field == CT_FIELD_STATES_THETA_MAX   ? b.theta_max
+                         : field == CT_FIELD_STATES_PHI_MAX     ? b.phi_max
+                                                                : b.activation_ms;
+      return copy_down(scn, dst, src, nbytes);  // written in reference voxel order
+    }
+    case CT_FIELD_SNAPSHOT_GAINS:
+    case CT_FIELD_SNAPSHOT_COEFS:
+    case CT_FIELD_SNAPSHOT_DELAYS:
+    case CT_FIELD_SNAPSHOT_SYSTEM_STATES: {
+      for (int64_t i = 0; i < scn->snap_n; ++i) {
+        int r = CT_OK;
+        if (field == CT_FIELD_SNAPSHOT_GAINS) {
+          const int64_t n = d.S * kGainCols;
+          r = copy_down_rows(scn, out + i * n, scn->snap_gains + i * n, 3, kGainCols);
+        } else if (field == CT_FIELD_SNAPSHOT_COEFS) {
+          const int64_t n = d.V * kOffsets;
+          r = copy_down_rows(scn, out + i * n, scn->snap_coefs + i * n, 1, kOffsets);
+        } else if (field == CT_FIELD_SNAPSHOT_DELAYS) {
+          const int64_t n = d.V * kOffsets;
+          r = copy_down_rows(scn, static_cast<int32_t*>(dst) + i * n, scn->snap_delays + i * n, 1, kOffsets);
+        } else {
+          const int64_t n = d.T * d.S;
+          r = copy_down_state_columns(scn, out + i * n, scn->snap_X + i * n, d.T);
+        }
+        if (r) return r;
+      }
+      return CT_OK;
+    }
+    case CT_FIELD_SNAPSHOT_MEASUREMENTS:
+      return scn->snap_n ? copy_down(scn, dst, scn->snap_Y, nbytes) : CT_OK;
     default: return fail(CT_ERR_INVALID_ARGUMENT, "unknown field %d", field);
   }
 }
@@ -1868,6 +1935,289 @@ int ct_batch_info(ct_batch* b, int64_t* graph_kernels, int* uses_graph) {
   if (graph_kernels) *graph_kernels = b->graph_kernels;
   if (uses_graph) *uses_graph = b->exec != nullptr ? 1 : 0;
   return CT_OK;
+}
+
+}  // extern "C"
+
+// ---- the callers either side of the epoch: the scenario loop and the post-run metrics
+
+namespace {
+
+static_assert(sizeof(ct_final_metrics) == sizeof(float) * (4 * CT_THRESHOLDS + 5),
+              "ct_final_metrics is a plain float array on the device");
+
+// Post-run buffers: the scan partials always, the spherical arrays when `arrays`.
+int ensure_post(ct_scn* s, bool arrays) {
+  DeviceScenario& d = s->d;
+  ct::PostBuffers& b = s->post;
+  int rc = CT_OK;
+  if (!b.inv) {
+    s->post_plan = ct::post_plan(d.V, d.T, s->ctx->num_sms);
+    const int64_t np = (int64_t)s->post_plan.parts * d.V;
+    if (!rc) rc = alloc(s, &b.inv, d.V);
+    if (!rc) rc = upload(s, b.inv, s->inv.data(), sizeof(int32_t) * (size_t)d.V);
+    if (!rc) rc = alloc(s, &b.maxmag, d.V);
+    if (!rc) rc = alloc(s, &b.part_val, np);
+    if (!rc) rc = alloc(s, &b.part_idx, np);
+    if (rc) {
+      release(s, b.inv);
+      release(s, b.maxmag);
+      release(s, b.part_val);
+      release(s, b.part_idx);
+      b = ct::PostBuffers{};
+      return rc;
+    }
+  }
+  if (arrays && !b.mag) {
+    float** big[] = {&b.mag, &b.theta, &b.phi};
+    float** small[] = {&b.mag_max, &b.theta_max, &b.phi_max, &b.activation_ms};
+    for (float** p : big)
+      if (!rc) rc = alloc(s, p, d.T * d.V);
+    for (float** p : small)
+      if (!rc) rc = alloc(s, p, d.V);
+    if (rc) {
+      for (float** p : big) release(s, *p), *p = nullptr;
+      for (float** p : small) release(s, *p), *p = nullptr;
+    }
+  }
+  return rc;
+}
+
+// Snapshot slots for `n` snapshots (re-allocated only when more are needed).
+int ensure_snapshots(ct_scn* s, int64_t n) {
+  s->snap_n = 0;
+  if (n <= s->snap_cap) return CT_OK;
+  DeviceScenario& d = s->d;
+  release(s, s->snap_gains);
+  release(s, s->snap_coefs);
+  release(s, s->snap_delays);
+  release(s, s->snap_X);
+  release(s, s->snap_Y);
+  s->snap_gains = s->snap_coefs = s->snap_X = s->snap_Y = nullptr;
+  s->snap_delays = nullptr;
+  s->snap_cap = 0;
+  int rc = alloc(s, &s->snap_gains, n * d.S * kGainCols);
+  if (!rc) rc = alloc(s, &s->snap_coefs, n * d.V * kOffsets);
+  if (!rc) rc = alloc(s, &s->snap_delays, n * d.V * kOffsets);
+  if (!rc) rc = alloc(s, &s->snap_X, n * d.T * d.S);
+  if (!rc) rc = alloc(s, &s->snap_Y, n * d.B * d.T * d.M);
+  if (!rc) s->snap_cap = n;
+  return rc;
+}
+
+// Snapshots::push (results.rs:224-247): parameters after the epoch's update, states and predicted
+// measurements of its last beat, stored in slot `i` (device order, converted on read).
+int push_snapshot(ct_scn* s, int64_t i) {
+  DeviceScenario& d = s->d;
+  cudaStream_t st = s->ctx->stream;
+  const size_t f = sizeof(float);
+  CT_CUDA(cudaMemcpyAsync(s->snap_gains + i * d.S * kGainCols, d.gains, f * d.S * kGainCols,
+                          cudaMemcpyDeviceToDevice, st), "snapshot");
+  CT_CUDA(cudaMemcpyAsync(s->snap_coefs + i * d.V * kOffsets, d.coefs, f * d.V * kOffsets, cudaMemcpyDeviceToDevice, st),
+          "snapshot");
+  CT_CUDA(cudaMemcpyAsync(s->snap_delays + i * d.V * kOffsets, d.delays, sizeof(int32_t) * d.V * kOffsets,
+                          cudaMemcpyDeviceToDevice, st), "snapshot");
+  CT_CUDA(cudaMemcpyAsync(s->snap_X + i * d.T * d.S, d.X, f * d.T * d.S, cudaMemcpyDeviceToDevice, st), "snapshot");
+  CT_CUDA(cudaMemcpyAsync(s->snap_Y + i * d.B * d.T * d.M, d.Y, f * d.B * d.T * d.M, cudaMemcpyDeviceToDevice, st),
+          "snapshot");
+  return CT_OK;
+}
+
+// Enqueues the read-back of the three batch losses at slot batch_index - 1 (the summary fields
+// run_model_based copies after every epoch, scenario.rs:753-756).
+int enqueue_summary_read(ct_scn* s, int64_t batch_index, float* out3) {
+  DeviceScenario& d = s->d;
+  if (batch_index < 1 || batch_index > d.NB)
+    return fail(CT_ERR_BATCH_INDEX, "batch index %lld outside the %lld slots", (long long)batch_index, (long long)d.NB);
+  cudaStream_t st = s->ctx->stream;
+  const int64_t i = batch_index - 1;
+  CT_CUDA(cudaMemcpyAsync(out3 + 0, d.loss_b + i, sizeof(float), cudaMemcpyDeviceToHost, st), "summary");
+  CT_CUDA(cudaMemcpyAsync(out3 + 1, d.loss_mse_b + i, sizeof(float), cudaMemcpyDeviceToHost, st), "summary");
+  CT_CUDA(cudaMemcpyAsync(out3 + 2, d.loss_mr_b + i, sizeof(float), cudaMemcpyDeviceToHost, st), "summary");
+  return CT_OK;
+}
+
+int check_run_config(const ct_run_config* c) {
+  if (c->epochs < 0) return fail(CT_ERR_INVALID_ARGUMENT, "negative epochs");
+  if (c->learning_rate_reduction_interval < 0) return fail(CT_ERR_INVALID_ARGUMENT, "negative reduction interval");
+  if (c->snapshots_interval < 0) return fail(CT_ERR_INVALID_ARGUMENT, "negative snapshots interval");
+  return CT_OK;
+}
+
+// Learning rate of epoch `e` given the running rate of epoch e-1 (scenario.rs:737-747).
+float scheduled_rate(const ct_run_config* c, int64_t e, float running, float original) {
+  float lr = running;
+  if (e == 0)
+    lr = 0.0f;
+  else if (e == 1)
+    lr = original;
+  if (c->learning_rate_reduction_interval != 0 && e % c->learning_rate_reduction_interval == 0)
+    lr = lr * c->learning_rate_reduction_factor;
+  return lr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ct_run_model_based(ct_scn* scn, const ct_run_config* cfg, const int32_t* beat_orders, int64_t* batch_index,
+                       float* epoch_losses, ct_run_summary* summary) {
+  if (!scn || !cfg || !batch_index || !summary) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  int rc = check_run_config(cfg);
+  if (rc) return rc;
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  *summary = ct_run_summary{};
+  const int64_t nsnap = cfg->snapshots_interval == 0 ? 0 : cfg->epochs / cfg->snapshots_interval + 1;
+  rc = ensure_snapshots(scn, nsnap);
+  if (rc) return rc;
+  const float original = scn->algo.learning_rate;
+  float lr = original;
+  float host[3] = {0.0f, 0.0f, 0.0f};
+  for (int64_t e = 0; e < cfg->epochs && !rc; ++e) {
+    lr = scheduled_rate(cfg, e, lr, original);
+    ct_set_learning_rate(scn, lr);
+    const int32_t* order = beat_orders ? beat_orders + e * scn->d.B : nullptr;
+    rc = ct_run_epoch(scn, batch_index, order, cfg->grad_mode, cfg->precision);
+    if (!rc) rc = enqueue_summary_read(scn, *batch_index, host);
+    const bool snap = cfg->snapshots_interval != 0 && e % cfg->snapshots_interval == 0;
+    if (!rc && snap) rc = push_snapshot(scn, scn->snap_n);
+    if (!rc) rc = ct_sync(scn);
+    if (rc) break;
+    if (snap) scn->snap_n += 1;
+    summary->epochs_run = e + 1;
+    summary->loss = host[0];
+    summary->loss_mse = host[1];
+    summary->loss_maximum_regularization = host[2];
+    if (epoch_losses) std::memcpy(epoch_losses + 3 * e, host, sizeof(host));
+    if (!std::isnormal(host[0])) break;  // the algorithm diverged (scenario.rs:778-781)
+  }
+  summary->snapshots = scn->snap_n;
+  ct_set_learning_rate(scn, original);
+  if (rc) return rc;
+  // calculate_average_delays of the final parameters (scenario.rs:783-790)
+  CT_CUDA(ct::launch_average_delays(scn->d, scn->ctx->stream), "average delays kernel");
+  scn->launches += 1;
+  return ct_sync(scn);
+}
+
+int ct_batch_run_model_based(ct_batch* batch, const ct_run_config* cfg, int64_t* batch_indices, float* epoch_losses,
+                             ct_run_summary* summaries) {
+  if (!batch || !cfg || !batch_indices || !summaries) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  int rc = check_run_config(cfg);
+  if (rc) return rc;
+  if (cfg->snapshots_interval != 0) return fail(CT_ERR_NOT_SUPPORTED, "batched runs store no snapshots");
+  if (cfg->grad_mode != batch->grad_mode || cfg->precision != batch->precision)
+    return fail(CT_ERR_INVALID_ARGUMENT, "the batch was created with another gradient mode or precision");
+  CT_CUDA(cudaSetDevice(batch->ctx->device), "cudaSetDevice");
+  const size_t n = batch->scns.size();
+  std::vector<float> original(n), lr(n), host(3 * n, 0.0f);
+  for (size_t i = 0; i < n; ++i) {
+    original[i] = lr[i] = batch->scns[i]->algo.learning_rate;
+    summaries[i] = ct_run_summary{};
+  }
+  std::vector<size_t> members(n);  // batch member index of each scenario of `cur`
+  for (size_t i = 0; i < n; ++i) members[i] = i;
+  ct_batch* cur = batch;
+  ct_batch* sub = nullptr;  // smaller batch once a member has stopped
+  std::vector<int64_t> idx;
+  for (int64_t e = 0; e < cfg->epochs && !rc && !members.empty(); ++e) {
+    for (size_t i : members) {
+      lr[i] = scheduled_rate(cfg, e, lr[i], original[i]);
+      ct_set_learning_rate(batch->scns[i], lr[i]);
+    }
+    idx.resize(members.size());
+    for (size_t k = 0; k < members.size(); ++k) idx[k] = batch_indices[members[k]];
+    rc = ct_batch_run_epoch(cur, idx.data());
+    for (size_t k = 0; k < members.size() && !rc; ++k) {
+      batch_indices[members[k]] = idx[k];
+      rc = enqueue_summary_read(batch->scns[members[k]], idx[k], host.data() + 3 * members[k]);
+    }
+    if (!rc) rc = ct_batch_sync(cur);
+    if (rc) break;
+    std::vector<size_t> still;
+    for (size_t i : members) {
+      const float* h = host.data() + 3 * i;
+      summaries[i].epochs_run = e + 1;
+      summaries[i].loss = h[0];
+      summaries[i].loss_mse = h[1];
+      summaries[i].loss_maximum_regularization = h[2];
+      if (epoch_losses) std::memcpy(epoch_losses + (i * (size_t)cfg->epochs + (size_t)e) * 3, h, 3 * sizeof(float));
+      if (std::isnormal(h[0])) still.push_back(i);
+    }
+    if (still.size() != members.size() && !still.empty() && e + 1 < cfg->epochs) {
+      // members whose loss stopped being normal leave; the others go on as a smaller batch
+      std::vector<ct_scn*> scns;
+      for (size_t i : still) scns.push_back(batch->scns[i]);
+      ct_batch* nb = nullptr;
+      rc = ct_batch_create(batch->ctx, scns.data(), (int64_t)scns.size(), batch->grad_mode, batch->precision, &nb);
+      if (!rc) {
+        nb->ckpt_k = batch->ckpt_k;
+        nb->tile_order = batch->tile_order;
+        rc = batch_build_tiles(nb, true);
+      }
+      if (sub) ct_batch_destroy(sub);
+      sub = nb;
+      cur = nb;
+    }
+    members.swap(still);
+  }
+  if (sub) ct_batch_destroy(sub);
+  for (size_t i = 0; i < n; ++i) ct_set_learning_rate(batch->scns[i], original[i]);
+  if (rc) return rc;
+  for (ct_scn* s : batch->scns) {
+    CT_CUDA(ct::launch_average_delays(s->d, s->ctx->stream), "average delays kernel");
+    s->launches += 1;
+  }
+  return ct_batch_sync(batch);
+}
+
+int ct_calculate_plotting_arrays(ct_scn* scn, float sample_rate_hz) {
+  if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  int rc = ensure_post(scn, true);
+  if (rc) return rc;
+  CT_CUDA(ct::launch_spherical(scn->d, scn->post, scn->post_plan, true, sample_rate_hz, scn->ctx->stream),
+          "spherical kernels");
+  scn->launches += 2;
+  rc = ct_sync(scn);
+  if (rc == CT_OK || rc == CT_ERR_NO_MAXIMUM) scn->post_arrays = true;
+  return rc;
+}
+
+int ct_calculate_final(ct_scn* scn, const int32_t* ground_truth_types, const int32_t* voxel_numbers, int64_t nx,
+                       int64_t ny, int64_t nz, ct_final_metrics* out) {
+  if (!scn || !ground_truth_types || !voxel_numbers || !out) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (nx <= 0 || ny <= 0 || nz <= 0) return fail(CT_ERR_INVALID_ARGUMENT, "empty grid");
+  const int64_t cells = nx * ny * nz;
+  const DeviceScenario& d = scn->d;
+  for (int64_t g = 0; g < cells; ++g) {
+    const int32_t num = voxel_numbers[g];
+    if (num != -1 && (num < 0 || num >= d.S || num % 3 != 0))
+      return fail(CT_ERR_INVALID_ARGUMENT, "voxel number %d of cell %lld is not a state index of this scenario",
+                  num, (long long)g);
+  }
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  int rc = ensure_post(scn, false);
+  if (rc) return rc;
+  cudaStream_t st = scn->ctx->stream;
+  const size_t grid_bytes = sizeof(int32_t) * (size_t)cells;
+  const size_t hist_bytes = sizeof(unsigned long long) * 2 * (CT_THRESHOLDS + 1);
+  char* tmp = nullptr;
+  CT_CUDA(cudaMallocAsync((void**)&tmp, hist_bytes + 2 * grid_bytes + sizeof(ct_final_metrics), st), "cudaMallocAsync");
+  unsigned long long* hist = reinterpret_cast<unsigned long long*>(tmp);
+  int32_t* types = reinterpret_cast<int32_t*>(tmp + hist_bytes);
+  int32_t* numbers = types + cells;
+  float* res = reinterpret_cast<float*>(tmp + hist_bytes + 2 * grid_bytes);
+  cudaError_t e = cudaMemcpyAsync(types, ground_truth_types, grid_bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(numbers, voxel_numbers, grid_bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = ct::launch_spherical(d, scn->post, scn->post_plan, false, 1.0f, st);
+  if (e == cudaSuccess)
+    e = ct::launch_final_metrics(scn->post, types, numbers, cells, hist, res, scn->ctx->num_sms, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, res, sizeof(ct_final_metrics), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(tmp, st);
+  if (e != cudaSuccess) return cuda_fail(e, "final metrics");
+  scn->launches += 4;
+  return ct_sync(scn);
 }
 
 }  // extern "C"

@@ -239,4 +239,33 @@ cudaError_t launch_expand_rows(const float* src, float* dst, int64_t V, cudaStre
 // Last-step maximum regularisation [S] from X[T-1].
 cudaError_t launch_last_max_reg(DeviceScenario& d, float threshold, float* out, cudaStream_t stream);
 
+// ---- post-run arrays and segmentation metrics (ct_post.cu)
+struct PostPlan {
+  int parts = 1;           // blocks of steps each voxel's scan is split into
+  int steps_per_part = 1;
+};
+PostPlan post_plan(int64_t V, int64_t T, int sms);
+// Device buffers of the post-run pass; the spherical arrays are reference voxel order.
+struct PostBuffers {
+  int32_t* inv = nullptr;          // [V] device voxel of each reference voxel
+  float* mag = nullptr;            // [T,V] |x| + |y| + |z|
+  float* theta = nullptr;          // [T,V]
+  float* phi = nullptr;            // [T,V]
+  float* mag_max = nullptr;        // [V] at the first maximum of the magnitude
+  float* theta_max = nullptr;      // [V]
+  float* phi_max = nullptr;        // [V]
+  float* activation_ms = nullptr;  // [V]
+  float* maxmag = nullptr;         // [V] largest magnitude, NaN when every step is NaN
+  float* part_val = nullptr;       // [parts,V] per block of steps: largest magnitude
+  int32_t* part_idx = nullptr;     // [parts,V] and its first step (-1: all NaN)
+};
+// Scan of X: maxmag always; with `write`, the spherical arrays, their maxima and the activation
+// times (a voxel whose magnitude is NaN at every step sets CT_ERR_NO_MAXIMUM in d.status).
+cudaError_t launch_spherical(const DeviceScenario& d, const PostBuffers& b, const PostPlan& plan, bool write,
+                             float sample_rate_hz, cudaStream_t stream);
+// Threshold sweep over `cells` grid cells (types, numbers in grid order) into `out`
+// (the ct_final_metrics layout); hist is 2 x (CT_THRESHOLDS + 1) device counters.
+cudaError_t launch_final_metrics(const PostBuffers& b, const int32_t* types, const int32_t* numbers, int64_t cells,
+                                 unsigned long long* hist, float* out, int sms, cudaStream_t stream);
+
 }  // namespace ct

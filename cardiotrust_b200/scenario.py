@@ -111,7 +111,7 @@ def from_coef_to_samples(coef) -> np.float32:
 
 @dataclasses.dataclass
 class ScenarioSpec:
-    """What to build. Sizes follow the workload descriptions in DESIGN.md."""
+    """What to build; the named workloads are in :func:`workload_spec`."""
 
     shape: tuple = (8, 8, 8)
     mask: str = "cuboid"  # "cuboid" | "shell"

@@ -16,6 +16,10 @@
  *                            (mutated by the caller's schedule, src/core/scenario.rs:737-747)
  *   ct_simulate           <- Simulation::run (forward)    src/core/data/simulation.rs:129-150
  *   ct_ctx_create         <- GPU::new                     src/core/algorithm/gpu.rs:31-64
+ *   ct_run_model_based    <- run_model_based              src/core/scenario.rs:725-795
+ *   ct_calculate_plotting_arrays <- calculate_plotting_arrays (estimations) src/core/scenario.rs:636-690
+ *   ct_calculate_final    <- metrics::calculate_final     src/core/algorithm/metrics.rs:226-242
+ *                            + optimal threshold summary  src/core/scenario.rs:601-617
  *
  * Conventions: every function returns a status (CT_OK = 0, negative CT_ERR_*),
  * never throws and never aborts. Host arrays passed in are copied; the caller
@@ -43,7 +47,8 @@ enum ct_status {
   CT_ERR_TIMEOUT = -4,          /* a device-side wait hit its iteration limit */
   CT_ERR_INVALID_INDEX = -5,    /* output_state_indices lack the voxel/neighbour structure */
   CT_ERR_NOT_SUPPORTED = -6,    /* mode not available for this scenario */
-  CT_ERR_BATCH_INDEX = -7       /* batch-wise metric index outside the metric arrays */
+  CT_ERR_BATCH_INDEX = -7,      /* batch-wise metric index outside the metric arrays */
+  CT_ERR_NO_MAXIMUM = -8        /* a voxel's magnitude is NaN at every step (argmax_skipnan finds none) */
 };
 
 /* Optimizer, src/core/algorithm/refinement.rs:8-12 */
@@ -133,7 +138,23 @@ enum ct_field {
   CT_FIELD_LOSS_MAXIMUM_REGULARIZATION = 42, /* [T] */
   CT_FIELD_LOSS_BATCH = 43,     /* [num_batch_slots] */
   CT_FIELD_LOSS_MSE_BATCH = 44,
-  CT_FIELD_LOSS_MAXIMUM_REGULARIZATION_BATCH = 45
+  CT_FIELD_LOSS_MAXIMUM_REGULARIZATION_BATCH = 45,
+  /* post-run arrays of the last beat's states, reference voxel order (read; written by
+   * ct_calculate_plotting_arrays, CT_ERR_INVALID_ARGUMENT before the first call) */
+  CT_FIELD_STATES_MAGNITUDE = 50,      /* [T,V] SystemStatesSpherical.magnitude, shapes.rs:151-192 */
+  CT_FIELD_STATES_THETA = 51,          /* [T,V] */
+  CT_FIELD_STATES_PHI = 52,            /* [T,V] */
+  CT_FIELD_STATES_MAGNITUDE_MAX = 53,  /* [V] SystemStatesSphericalMax, shapes.rs:242-277 */
+  CT_FIELD_STATES_THETA_MAX = 54,      /* [V] */
+  CT_FIELD_STATES_PHI_MAX = 55,        /* [V] */
+  CT_FIELD_ACTIVATION_TIMES = 56,      /* [V] ActivationTimePerStateMs, shapes.rs:322-352 */
+  /* snapshots of the last ct_run_model_based call (Snapshots, src/core/scenario/results.rs:179-248); N = the
+   * number of snapshots that call allocated (epochs / snapshots_interval + 1, 0 without) */
+  CT_FIELD_SNAPSHOT_GAINS = 60,        /* [N,S,78] */
+  CT_FIELD_SNAPSHOT_COEFS = 61,        /* [N,V,26] */
+  CT_FIELD_SNAPSHOT_DELAYS = 62,       /* [N,V,26] i32 */
+  CT_FIELD_SNAPSHOT_SYSTEM_STATES = 63,/* [N,T,S] */
+  CT_FIELD_SNAPSHOT_MEASUREMENTS = 64  /* [N,B,T,M] */
 };
 
 typedef struct ct_ctx ct_ctx;
@@ -244,6 +265,85 @@ int ct_set_profiling(ct_scn* scn, int enable);
 /* Accumulated device milliseconds and launch counts per phase (arrays of CT_PHASE_COUNT).
  * Synchronizes the context stream. */
 int ct_read_profile(ct_scn* scn, double* ms, int64_t* launches);
+
+/* ---- the scenario loop and the post-run metrics (the callers either side of the epoch) */
+
+/* Settings of the reference's epoch loop, run_model_based (src/core/scenario.rs:725-795), read from
+ * the Algorithm config (src/core/config/algorithm.rs:25-58). The learning rate is the scenario's
+ * (ct_set_learning_rate / the create-time algorithm): epoch 0 runs with learning rate 0, epoch 1
+ * restores it, and every epoch whose index is a multiple of learning_rate_reduction_interval
+ * (when non-zero) multiplies the running rate by learning_rate_reduction_factor. */
+typedef struct ct_run_config {
+  int64_t epochs;
+  int64_t learning_rate_reduction_interval; /* 0 = never */
+  float learning_rate_reduction_factor;
+  int32_t grad_mode;                        /* ct_grad_mode of every epoch */
+  int32_t precision;                        /* ct_precision of every epoch */
+  int64_t snapshots_interval;               /* 0 = no snapshots */
+} ct_run_config;
+
+/* The loss part of the reference's Summary (src/core/scenario/summary.rs:25-42) after the loop. */
+typedef struct ct_run_summary {
+  int64_t epochs_run; /* epochs executed: fewer than requested when the loss stopped being normal */
+  int64_t snapshots;  /* snapshots stored (CT_FIELD_SNAPSHOT_*) */
+  float loss;         /* loss_batch[batch_index - 1] of the last epoch run */
+  float loss_mse;
+  float loss_maximum_regularization;
+} ct_run_summary;
+
+/* run_model_based: cfg->epochs epochs of ct_run_epoch under the learning-rate schedule above; after
+ * each epoch the three batch losses of its last batch are read back (the summary the reference
+ * sends per epoch), a snapshot is stored when the epoch index is a multiple of snapshots_interval,
+ * and the loop stops early when the loss is not a normal number (zero, subnormal, infinite or
+ * NaN: f32::is_normal). Then the average delays are recomputed from the final parameters
+ * (CT_FIELD_AVERAGE_DELAYS) and the scenario's learning rate is restored. Synchronous.
+ * beat_orders: [epochs, B] beat orders, or NULL for the library's seeded shuffle each epoch.
+ * batch_index: in/out as for ct_run_epoch. epoch_losses: NULL or [epochs, 3] (loss, loss_mse,
+ * loss_maximum_regularization per epoch run; rows of epochs not run are left untouched). */
+int ct_run_model_based(ct_scn* scn, const ct_run_config* cfg, const int32_t* beat_orders, int64_t* batch_index,
+                       float* epoch_losses, ct_run_summary* summary);
+
+/* The same loop over every member of a batch (one ct_batch_run_epoch per epoch; beats in index
+ * order). Each member follows its own learning rate through the schedule and stops on its own
+ * non-normal loss; the remaining members continue as a smaller batch. No snapshots
+ * (snapshots_interval must be 0). batch_indices: in/out per member. epoch_losses: NULL or
+ * [count, epochs, 3]. summaries: [count]. Synchronous. */
+int ct_batch_run_model_based(ct_batch* batch, const ct_run_config* cfg, int64_t* batch_indices, float* epoch_losses,
+                             ct_run_summary* summaries);
+
+/* calculate_plotting_arrays (src/core/scenario.rs:636-690), estimation side: from the last beat's
+ * states, the spherical arrays (magnitude |x|+|y|+|z|, theta = acos(z / magnitude),
+ * phi = atan2(y, x)), their values at each voxel's first maximum of the magnitude, and the
+ * activation time (that step / sample_rate_hz * 1000, ms). Results in CT_FIELD_STATES_* and
+ * CT_FIELD_ACTIVATION_TIMES. CT_ERR_NO_MAXIMUM when a voxel's magnitude is NaN at every step
+ * (the reference's argmax_skipnan error). The differences against the simulation's arrays are the
+ * same call on the ground-truth scenario followed by a subtraction. Synchronous. */
+int ct_calculate_plotting_arrays(ct_scn* scn, float sample_rate_hz);
+
+#define CT_THRESHOLDS 101
+/* Metrics::*_over_threshold (src/core/algorithm/metrics.rs:20-37) and the Summary fields chosen at
+ * the Dice-optimal threshold (src/core/scenario.rs:601-617). */
+typedef struct ct_final_metrics {
+  float dice_score_over_threshold[CT_THRESHOLDS]; /* threshold i / 100, i = 0..100 */
+  float iou_over_threshold[CT_THRESHOLDS];
+  float precision_over_threshold[CT_THRESHOLDS];
+  float recall_over_threshold[CT_THRESHOLDS];
+  float threshold; /* first threshold of the largest Dice score */
+  float dice;
+  float iou;
+  float recall;
+  float precision;
+} ct_final_metrics;
+
+/* metrics::calculate_final (src/core/algorithm/metrics.rs:226-447): a grid cell with a voxel number
+ * is predicted pathological at threshold t when the largest magnitude of its voxel's last-beat
+ * states over all steps (NaN steps skipped) is <= t; Dice, IoU, precision and recall against the
+ * ground truth for t = 0, 0.01, ..., 1, and the summary at the Dice-optimal threshold.
+ * ground_truth_types: [nx,ny,nz] VoxelType discriminants (voxels.rs:664-676, Pathological = 6) of
+ * the simulation; voxel_numbers: [nx,ny,nz] state index of each cell's voxel (multiple of 3, < S)
+ * or -1 (None), of the estimated model. Synchronous. */
+int ct_calculate_final(ct_scn* scn, const int32_t* ground_truth_types, const int32_t* voxel_numbers, int64_t nx,
+                       int64_t ny, int64_t nz, ct_final_metrics* out);
 
 /* Allocation-free H x product for callers that must not see this library allocate device
  * memory: hosts that keep every device buffer in their own pool or arena or run under a fixed

@@ -218,6 +218,83 @@ class OracleEpoch:
         return self.measurements.copy()
 
 
+    def run_model_based(self, algo: Algo, epochs: int, learning_rate_reduction_interval: int = 0,
+                        learning_rate_reduction_factor: float = 0.0, snapshots_interval: int = 0,
+                        beat_orders=None, adjoint: bool = False):
+        """``run_model_based`` (src/core/scenario.rs:725-795): learning rate 0 in epoch 0, restored in
+        epoch 1, multiplied by the factor at every multiple of the interval; the batch losses of the
+        last batch after every epoch; a snapshot (results.rs:224-247) at every multiple of the
+        snapshot interval; stop when the loss is not a normal number; average delays of the final
+        parameters. Returns (summary dict, [epochs_run, 3] losses, snapshots dict of lists)."""
+        original = np.float32(algo.learning_rate)
+        lr = original
+        losses = []
+        snaps = {"gains": [], "coefs": [], "delays": [], "system_states": [], "measurements": []}
+        summary = dict(epochs_run=0, loss=0.0, loss_mse=0.0, loss_maximum_regularization=0.0)
+        for e in range(int(epochs)):
+            if e == 0:
+                lr = np.float32(0.0)
+            elif e == 1:
+                lr = original
+            if learning_rate_reduction_interval != 0 and e % learning_rate_reduction_interval == 0:
+                lr = np.float32(lr * np.float32(learning_rate_reduction_factor))
+            algo.learning_rate = float(lr)
+            self.run_epoch(algo, beat_order=None if beat_orders is None else beat_orders[e], adjoint=adjoint)
+            i = self.batch_index - 1
+            row = (self.loss_batch[i], self.loss_mse_batch[i], self.loss_maximum_regularization_batch[i])
+            summary.update(epochs_run=e + 1, loss=float(row[0]), loss_mse=float(row[1]),
+                           loss_maximum_regularization=float(row[2]))
+            losses.append(row)
+            if snapshots_interval != 0 and e % snapshots_interval == 0:
+                snaps["gains"].append(self.gains.copy())
+                snaps["coefs"].append(self.coefs.copy())
+                snaps["delays"].append(self.delays.copy())
+                snaps["system_states"].append(self.system_states.copy())
+                snaps["measurements"].append(self.measurements.copy())
+            loss = np.float32(row[0])
+            if not (np.isfinite(loss) and abs(loss) >= np.finfo(np.float32).tiny):  # f32::is_normal
+                break
+        algo.learning_rate = float(original)
+        s = self._struct()
+        lib().oracle_average_delays_f32(ctypes.byref(s))
+        return summary, np.array(losses, dtype=self.dtype).reshape(-1, 3), snaps
+
+
+def plotting_arrays(system_states: np.ndarray, sample_rate_hz: float):
+    """Estimation side of ``calculate_plotting_arrays`` (src/core/scenario.rs:636-690): spherical
+    arrays [T,V], their values at each voxel's first magnitude maximum and activation times [V].
+    Returns (dict of arrays, status: 0, or -8 when some voxel is NaN at every step)."""
+    X = np.ascontiguousarray(system_states, dtype=np.float32)
+    T, S = X.shape
+    V = S // 3
+    out = {k: np.empty((T, V), np.float32) for k in ("magnitude", "theta", "phi")}
+    out.update({k: np.empty(V, np.float32) for k in ("magnitude_max", "theta_max", "phi_max", "activation_times")})
+    fn = lib().oracle_plotting_arrays_f32
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_float] + [ctypes.c_void_p] * 7
+    rc = fn(X.ctypes.data, T, S, float(sample_rate_hz), *[out[k].ctypes.data for k in (
+        "magnitude", "theta", "phi", "magnitude_max", "theta_max", "phi_max", "activation_times")])
+    return out, int(rc)
+
+
+def calculate_final(system_states: np.ndarray, ground_truth_types: np.ndarray, voxel_numbers: np.ndarray) -> dict:
+    """``metrics::calculate_final`` (src/core/algorithm/metrics.rs:226-447) and the Dice-optimal
+    summary (src/core/scenario.rs:601-617), restated literally (one voxel-type prediction per
+    threshold)."""
+    X = np.ascontiguousarray(system_states, dtype=np.float32)
+    gt = np.ascontiguousarray(ground_truth_types, dtype=np.int32)
+    nums = np.ascontiguousarray(voxel_numbers, dtype=np.int32)
+    out = np.empty(4 * 101 + 5, np.float32)
+    fn = lib().oracle_calculate_final_f32
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                   ctypes.c_int64, ctypes.c_void_p]
+    fn(X.ctypes.data, X.shape[0], X.shape[1], gt.ctypes.data, nums.ctypes.data, gt.size, out.ctypes.data)
+    keys = ("threshold", "dice", "iou", "recall", "precision")
+    res = dict(dice_score_over_threshold=out[0:101], iou_over_threshold=out[101:202],
+               precision_over_threshold=out[202:303], recall_over_threshold=out[303:404])
+    res.update({k: float(out[404 + i]) for i, k in enumerate(keys)})
+    return res
+
+
 def algo(**kw) -> Algo:
     """An Algo with the reference defaults (config/algorithm.rs:59-85), overridden by ``kw``."""
     a = Algo()

@@ -782,9 +782,129 @@ T adjoint_gradient(Epoch<T>& e, const Algo& a, bool want_grad) {
   return loss;
 }
 
+// ---- post-run arrays and segmentation metrics (the callers after the epoch loop)
+
+// SystemStatesSpherical::calculate (src/core/data/shapes.rs:171-192): magnitude, theta, phi [T,V].
+void spherical(const float* X, int64_t T, int64_t S, float* mag, float* theta, float* phi) {
+  const int64_t V = S / 3;
+  for (int64_t t = 0; t < T; ++t)
+    for (int64_t v = 0; v < V; ++v) {
+      const float* x = X + t * S + 3 * v;
+      mag[t * V + v] = std::fabs(x[0]) + std::fabs(x[1]) + std::fabs(x[2]);
+    }
+  for (int64_t t = 0; t < T; ++t)
+    for (int64_t v = 0; v < V; ++v) theta[t * V + v] = std::acos(X[t * S + 3 * v + 2] / mag[t * V + v]);
+  for (int64_t t = 0; t < T; ++t)
+    for (int64_t v = 0; v < V; ++v) phi[t * V + v] = std::atan2(X[t * S + 3 * v + 1], X[t * S + 3 * v]);
+}
+
+// ndarray-stats 0.6.0 `argmax_skipnan` over column v of a [T,V] array: index of the first of the
+// largest non-NaN values; -1 when every value is NaN (the crate's MinMaxError::EmptyInput).
+int64_t argmax_skipnan_col(const float* a, int64_t T, int64_t V, int64_t v) {
+  int64_t best = -1;
+  for (int64_t t = 0; t < T; ++t) {
+    const float x = a[t * V + v];
+    if (std::isnan(x)) continue;
+    if (best < 0 || x > a[best * V + v]) best = t;
+  }
+  return best;
+}
+
+// ndarray-stats 0.6.0 `max_skipnan` of a 1-d array: largest non-NaN value, NaN if there is none.
+float max_skipnan(const std::vector<float>& a) {
+  bool any = false;
+  float m = 0.0f;
+  for (float x : a) {
+    if (std::isnan(x)) continue;
+    if (!any || x > m) m = x;
+    any = true;
+  }
+  return any ? m : std::nanf("");
+}
+
+constexpr int kVoxelNone = 0, kVoxelVentricle = 5, kVoxelPathological = 6;  // voxels.rs:664-676
+
+// predict_voxeltype (metrics.rs:409-447)
+void predict_voxeltype(const float* X, int64_t T, int64_t S, const int32_t* numbers, int64_t cells, float threshold,
+                       int32_t* pred) {
+  std::vector<float> abs((size_t)T);
+  for (int64_t g = 0; g < cells; ++g) {
+    pred[g] = kVoxelNone;
+    const int32_t n = numbers[g];
+    if (n < 0) continue;
+    for (int64_t t = 0; t < T; ++t)
+      abs[(size_t)t] = std::fabs(X[t * S + n]) + std::fabs(X[t * S + n + 1]) + std::fabs(X[t * S + n + 2]);
+    pred[g] = max_skipnan(abs) <= threshold ? kVoxelPathological : kVoxelVentricle;
+  }
+}
+
+// calculate_dice / calculate_iou / calculate_precision / calculate_recall (metrics.rs:268-399)
+void segmentation_scores(const int32_t* pred, const int32_t* gt, int64_t cells, float* dice, float* iou,
+                         float* precision, float* recall) {
+  size_t tp = 0, fp = 0, fn = 0, gt_pos = 0, pred_pos = 0, uni = 0;
+  for (int64_t g = 0; g < cells; ++g) {
+    const bool p = pred[g] == kVoxelPathological, q = gt[g] == kVoxelPathological;
+    tp += p && q;
+    fp += p && !q;
+    fn += !p && q;
+    gt_pos += q;
+    pred_pos += p;
+    uni += p || q;
+  }
+  const size_t den = 2 * tp + fp + fn;
+  *dice = den == 0 ? 0.0f : static_cast<float>(2 * tp) / static_cast<float>(den);
+  *iou = uni == 0 ? 0.0f : static_cast<float>(tp) / static_cast<float>(uni);
+  *precision = pred_pos == 0 ? 0.0f : static_cast<float>(tp) / static_cast<float>(pred_pos);
+  *recall = gt_pos == 0 ? 1.0f : static_cast<float>(tp) / static_cast<float>(gt_pos);
+}
+
 }  // namespace
 
 extern "C" {
+
+// calculate_plotting_arrays, estimation side (scenario.rs:636-690 with shapes.rs:171-192,262-277,
+// 334-352). Returns 0, or -8 when a voxel's magnitude is NaN at every step (argmax_skipnan fails;
+// that voxel's maxima are left NaN).
+int oracle_plotting_arrays_f32(const float* X, int64_t T, int64_t S, float sample_rate_hz, float* mag, float* theta,
+                               float* phi, float* mag_max, float* theta_max, float* phi_max, float* activation_ms) {
+  const int64_t V = S / 3;
+  spherical(X, T, S, mag, theta, phi);
+  int rc = 0;
+  for (int64_t v = 0; v < V; ++v) {
+    const int64_t i = argmax_skipnan_col(mag, T, V, v);
+    if (i < 0) {
+      rc = -8;
+      mag_max[v] = theta_max[v] = phi_max[v] = activation_ms[v] = std::nanf("");
+      continue;
+    }
+    mag_max[v] = mag[i * V + v];
+    theta_max[v] = theta[i * V + v];
+    phi_max[v] = phi[i * V + v];
+    activation_ms[v] = static_cast<float>(i) / sample_rate_hz * 1000.0f;
+  }
+  return rc;
+}
+
+// metrics::calculate_final (metrics.rs:226-242) and the Dice-optimal summary (scenario.rs:601-617).
+// out: dice[101], iou[101], precision[101], recall[101], threshold, dice, iou, recall, precision.
+void oracle_calculate_final_f32(const float* X, int64_t T, int64_t S, const int32_t* gt, const int32_t* numbers,
+                                int64_t cells, float* out) {
+  std::vector<int32_t> pred((size_t)cells);
+  for (int i = 0; i <= 100; ++i) {
+    const float threshold = static_cast<float>(i) / 100.0f;
+    predict_voxeltype(X, T, S, numbers, cells, threshold, pred.data());
+    segmentation_scores(pred.data(), gt, cells, out + i, out + 101 + i, out + 202 + i, out + 303 + i);
+  }
+  int best = -1;
+  for (int i = 0; i <= 100; ++i)
+    if (!std::isnan(out[i]) && (best < 0 || out[i] > out[best])) best = i;
+  if (best < 0) best = 0;  // unwrap_or_default()
+  out[404] = static_cast<float>(best) / 100.0f;
+  out[405] = out[best];
+  out[406] = out[101 + best];
+  out[407] = out[303 + best];
+  out[408] = out[202 + best];
+}
 
 int oracle_abi_version() { return 1; }
 
