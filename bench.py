@@ -21,6 +21,7 @@ seed), no data-path collective; time = max over ranks.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import pathlib
@@ -79,16 +80,27 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.skip = 0
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "50",
                  "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        # the timed region starts once the sampler is producing lines (nvidia-smi takes ~0.1-0.5 s to start)
+        t0 = time.perf_counter()
+        while not self.lines and time.perf_counter() - t0 < 3.0:
+            time.sleep(0.01)
+        self.skip = len(self.lines)
+
+    def mark(self):
+        """Samples from here on count (the timed region starts)."""
+        self.skip = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -104,7 +116,7 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for line in self.lines[self.skip:]:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 8:
                 continue
@@ -267,6 +279,57 @@ def forms_section(alg, eng, bi, prec, stream, flush, scn):
     return out
 
 
+def post_run_section(alg, eng, scn, stream, hbm_peak, prec):
+    """The callers either side of the epoch on the headline workload: the post-run pass (spherical
+    arrays of the last beat, their maxima, activation times; then the 101-threshold segmentation
+    metrics) and the reference's epoch loop (learning-rate schedule, per-epoch summary read-back)."""
+    import torch
+
+    V, T = scn.num_voxels, scn.num_steps
+    sr = scn.spec.sample_rate_hz
+    eng.calculate_plotting_arrays(sr)
+    ms = []
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.calculate_plotting_arrays(sr)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    call_ms = min(ms)
+    algo_bytes = 24.0 * T * V  # 12 B of states read and 12 B of magnitude/theta/phi written per (step, voxel)
+    achieved = algo_bytes / (call_ms / 1000.0) / 1e9
+    t0 = time.perf_counter()
+    fm = eng.calculate_final(scn.types_truth, scn.numbers)
+    first_ms = (time.perf_counter() - t0) * 1000.0  # includes the one-time buffer set-up and kernel loading
+    fms = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        fm = eng.calculate_final(scn.types_truth, scn.numbers)
+        fms.append((time.perf_counter() - t0) * 1000.0)
+    final_ms = min(fms)
+    loop_epochs = 5
+    a = dataclasses.replace(algorithm_config(alg), epochs=loop_epochs, learning_rate_reduction_interval=2,
+                            learning_rate_reduction_factor=0.5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    # batch-metric slots from 0 again: only the timing and the epoch count are read
+    summ, _, _ = eng.run_model_based(0, precision=prec, algorithm=a)
+    loop_s = time.perf_counter() - t0
+    return {
+        "plotting_arrays": {"call_ms": call_ms, "algorithmic_bytes": algo_bytes, "achieved_gbs": achieved,
+                            "frac": achieved / hbm_peak,
+                            "note": "CUDA events around the synchronous C call (its device sync included)"},
+        "final_metrics": {"call_ms": final_ms, "first_call_ms": first_ms, "threshold": fm.threshold,
+                          "dice": fm.dice, "iou": fm.iou,
+                          "note": "wall clock of the C call (best of 5 after the first): grid upload, states scan, "
+                                  "threshold sweep, read-back"},
+        "scenario_loop": {"epochs": loop_epochs, "epochs_run": summ["epochs_run"],
+                          "scenario_epochs_per_s": loop_epochs / loop_s,
+                          "note": "ct_run_model_based wall clock: schedule, one summary read-back per epoch"},
+    }
+
+
 def batched_section(args, alg, sc, ctx, prec, stream, flush):
     """64 scenarios of uneven size (batch_workload_specs): the batched adjoint epoch (one forward and
     one adjoint launch per beat index over every member, replayed from a CUDA graph) against the plain
@@ -325,7 +388,7 @@ def batched_section(args, alg, sc, ctx, prec, stream, flush):
                                          "whose state count is a multiple of 4, fp32 for the others",
                    "scenario_epochs_per_s": chosen, "voxel_steps_per_s": vtb * 1000.0 / chosen_ms,
                    "ms_per_epoch": chosen_ms, "graph_kernels": info["graph_kernels"], "uses_graph": info["uses_graph"],
-                   "autotuned": tuned},
+                   "forward_ctas": info["forward_ctas"], "adjoint_ctas": info["adjoint_ctas"], "autotuned": tuned},
         "plain": {"form": "plain GPU form, one scenario at a time, one launch per phase per step (reference "
                           "gradients, FP32)", "scenario_epochs_per_s": plain,
                   "voxel_steps_per_s": vtb * 1000.0 / plain_ms, "ms_per_epoch_all": plain_ms},
@@ -475,15 +538,16 @@ def gpu_arm(args):
         if world > 1:
             torch.distributed.barrier()
 
+    clocks = ClockSampler(local_rank)
+    clocks.start()
     bi = 0
     for _ in range(args.warmup):
         bi = eng.run_epoch(bi, precision=prec, sync=True)
     barrier()
 
-    # ---- device-resident timed region
+    # ---- device-resident timed region (clock samples every 50 ms from here to its end)
     launches0 = eng.kernel_launches()
-    clocks = ClockSampler(local_rank)
-    clocks.start()
+    clocks.mark()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     for k in range(args.steps):
         flush.random_(0, 255)
@@ -560,21 +624,21 @@ def gpu_arm(args):
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch (profiles/)",
                 "algorithmic_bytes_per_launch": algo_bytes[rl_kernel], "launch_ms": per_launch_ms}
 
-    # ---- the precision report's f64 oracle runs on the host from here on, next to the GPU-only sections
-    # (after the end-to-end and CPU-sensitive measurements)
-    prec_job = None
-    if args.precision_steps > 0 and rank == 0 and world == 1:
-        prec_job = _Job(precision_cases, args.precision_steps)
-        prec_job.start()
-
-    # ---- plain GPU form and adjoint mode on the same workload; the batched workload
+    # ---- plain GPU form and adjoint mode on the same workload; the batched workload. The plain forms
+    # are launch-bound, so nothing else runs on the host while they are timed.
     forms = forms_section(alg, eng, bi, prec, stream, flush, scn)
+    post_run = post_run_section(alg, eng, scn, stream, hbm_peak, prec)
     batched = None
     if args.batch_scenarios > 0 and world == 1:
         eng.close()
         batched = batched_section(args, alg, sc, ctx, prec, stream, flush)
 
-    precision = precision_section(alg, ctx, prec_job) if prec_job is not None else None
+    # ---- precision report: the f64 oracle on the host, then the GPU products of the same cases
+    precision = None
+    if args.precision_steps > 0 and rank == 0 and world == 1:
+        prec_job = _Job(precision_cases, args.precision_steps)
+        prec_job.start()
+        precision = precision_section(alg, ctx, prec_job)
 
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
@@ -623,6 +687,7 @@ def gpu_arm(args):
             "forms": forms,
             "chosen_vs_plain": value / forms["plain"]["scenario_epochs_per_s"],
             "batched": batched,
+            "post_run": post_run,
             "precision": precision,
         }
         print(json.dumps(line), flush=True)

@@ -229,7 +229,8 @@ def load(path: pathlib.Path = LIB_PATH) -> ctypes.CDLL:
     lib.ct_batch_destroy.argtypes = [vp]
     lib.ct_batch_run_epoch.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     lib.ct_batch_sync.argtypes = [vp]
-    lib.ct_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int)]
+    lib.ct_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     lib.ct_batch_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.ct_batch_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]

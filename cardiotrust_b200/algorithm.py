@@ -403,9 +403,10 @@ class EpochBatch:
 
     def info(self) -> dict:
         k = ctypes.c_int64()
-        g = ctypes.c_int()
-        check(lib().ct_batch_info(self._h, ctypes.byref(k), ctypes.byref(g)))
-        return {"graph_kernels": int(k.value), "uses_graph": bool(g.value)}
+        g, f, a = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().ct_batch_info(self._h, ctypes.byref(k), ctypes.byref(g), ctypes.byref(f), ctypes.byref(a)))
+        return {"graph_kernels": int(k.value), "uses_graph": bool(g.value), "forward_ctas": int(f.value),
+                "adjoint_ctas": int(a.value)}
 
     def autotune(self) -> dict:
         """Time candidate schedules on real epochs (they train) and keep the fastest; see ct_batch_autotune."""

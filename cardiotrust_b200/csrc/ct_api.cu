@@ -73,6 +73,11 @@ struct ct_scn {
   ct::PostBuffers post{};
   ct::PostPlan post_plan{};
   bool post_arrays = false;  // CT_FIELD_STATES_* / CT_FIELD_ACTIVATION_TIMES hold results
+  // ct_calculate_final: grid types and numbers [2, cells], threshold histogram, results (grown on demand)
+  int64_t final_cells = 0;
+  int32_t* final_grid = nullptr;
+  unsigned long long* final_hist = nullptr;
+  float* final_out = nullptr;
   // snapshots of the last ct_run_model_based call: snap_n stored slots of snap_cap allocated
   int64_t snap_n = 0, snap_cap = 0;
   float* snap_gains = nullptr;
@@ -1930,10 +1935,12 @@ int ct_batch_read_profile(ct_batch* b, double* ms) {
   return CT_OK;
 }
 
-int ct_batch_info(ct_batch* b, int64_t* graph_kernels, int* uses_graph) {
+int ct_batch_info(ct_batch* b, int64_t* graph_kernels, int* uses_graph, int* forward_ctas, int* adjoint_ctas) {
   if (!b) return fail(CT_ERR_INVALID_ARGUMENT, "batch is NULL");
   if (graph_kernels) *graph_kernels = b->graph_kernels;
   if (uses_graph) *uses_graph = b->exec != nullptr ? 1 : 0;
+  if (forward_ctas) *forward_ctas = b->fwd_grid;
+  if (adjoint_ctas) *adjoint_ctas = b->adj_grid;
   return CT_OK;
 }
 
@@ -2199,22 +2206,31 @@ int ct_calculate_final(ct_scn* scn, const int32_t* ground_truth_types, const int
   CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
   int rc = ensure_post(scn, false);
   if (rc) return rc;
+  if (!scn->final_hist) {
+    rc = alloc(scn, &scn->final_hist, 2 * (CT_THRESHOLDS + 1));
+    if (!rc) rc = alloc(scn, &scn->final_out, (int64_t)(sizeof(ct_final_metrics) / sizeof(float)));
+    if (rc) return rc;
+  }
+  if (cells > scn->final_cells) {
+    release(scn, scn->final_grid);
+    scn->final_grid = nullptr;
+    scn->final_cells = 0;
+    rc = alloc(scn, &scn->final_grid, 2 * cells);
+    if (rc) return rc;
+    scn->final_cells = cells;
+  }
   cudaStream_t st = scn->ctx->stream;
   const size_t grid_bytes = sizeof(int32_t) * (size_t)cells;
-  const size_t hist_bytes = sizeof(unsigned long long) * 2 * (CT_THRESHOLDS + 1);
-  char* tmp = nullptr;
-  CT_CUDA(cudaMallocAsync((void**)&tmp, hist_bytes + 2 * grid_bytes + sizeof(ct_final_metrics), st), "cudaMallocAsync");
-  unsigned long long* hist = reinterpret_cast<unsigned long long*>(tmp);
-  int32_t* types = reinterpret_cast<int32_t*>(tmp + hist_bytes);
-  int32_t* numbers = types + cells;
-  float* res = reinterpret_cast<float*>(tmp + hist_bytes + 2 * grid_bytes);
+  int32_t* types = scn->final_grid;
+  int32_t* numbers = scn->final_grid + cells;
   cudaError_t e = cudaMemcpyAsync(types, ground_truth_types, grid_bytes, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(numbers, voxel_numbers, grid_bytes, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = ct::launch_spherical(d, scn->post, scn->post_plan, false, 1.0f, st);
   if (e == cudaSuccess)
-    e = ct::launch_final_metrics(scn->post, types, numbers, cells, hist, res, scn->ctx->num_sms, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(out, res, sizeof(ct_final_metrics), cudaMemcpyDeviceToHost, st);
-  cudaFreeAsync(tmp, st);
+    e = ct::launch_final_metrics(scn->post, types, numbers, cells, scn->final_hist, scn->final_out,
+                                 scn->ctx->num_sms, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, scn->final_out, sizeof(ct_final_metrics), cudaMemcpyDeviceToHost, st);
   if (e != cudaSuccess) return cuda_fail(e, "final metrics");
   scn->launches += 4;
   return ct_sync(scn);

@@ -222,8 +222,9 @@ int ct_batch_run_epoch(ct_batch* batch, int64_t* batch_indices);
 int ct_batch_autotune(ct_batch* batch, int64_t* batch_indices, int* ckpt_k, int* tile_order, double* best_ms);
 /* Waits for the batch and reports any device-side failure of a member. */
 int ct_batch_sync(ct_batch* batch);
-/* Kernel nodes in the captured epoch graph, and whether the graph is used (0: eager launches). */
-int ct_batch_info(ct_batch* batch, int64_t* graph_kernels, int* uses_graph);
+/* Kernel nodes in the captured epoch graph, whether the graph is used (0: eager launches), and the
+ * CTAs of the persistent forward and adjoint launches (all co-resident). NULL outputs are skipped. */
+int ct_batch_info(ct_batch* batch, int64_t* graph_kernels, int* uses_graph, int* forward_ctas, int* adjoint_ctas);
 /* Per-phase device time of batched epochs: while enabled, epochs run as eager launches (not the
  * graph) with CUDA events around each phase; ct_batch_read_profile waits for the batch and writes
  * CT_PHASE_COUNT totals in ms since enabling (FORWARD: memsets + forward launches; MEASURE: the

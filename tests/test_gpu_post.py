@@ -89,24 +89,24 @@ def test_plotting_arrays_nan_states(alg, ctx, oracle_mod, shell):
     eng.close()
 
 
-def _scaled(shell, factor):
-    """The same scenario with the control pulse scaled (states are linear in it)."""
-    import dataclasses
+@pytest.fixture(scope="module")
+def shell_front():
+    """The same shell with a 120-step beat: the activation front is part-way across, so the voxels'
+    maxima spread from 0 to 1 and the Dice score changes along the threshold sweep."""
+    from cardiotrust_b200 import scenario as sc
 
-    return dataclasses.replace(shell, control_function=(shell.control_function * np.float32(factor)).astype(np.float32))
+    spec = sc.ScenarioSpec(shape=(12, 11, 10), mask="shell", shell_semi_axes=(6.0, 5.5, 5.0), shell_thickness=2.0,
+                           num_steps=120, num_beats=2, patho_size=3, pulse_onset=2, pulse_sigma_samples=5.0,
+                           noise_fraction=0.01, seed=4)
+    return sc.build(spec)
 
 
-@pytest.mark.parametrize("case", ["as_built", "maxima_spread_over_thresholds", "nan_voxel"])
-def test_final_metrics_match_oracle(alg, ctx, oracle_mod, shell, case):
-    scn = shell
-    if case == "maxima_spread_over_thresholds":
-        probe = alg.EpochEngine.from_scenario(ctx, shell)
-        probe.simulate()
-        x = probe.read("system_states").reshape(shell.num_steps, -1, 3)
-        peak = np.abs(x).sum(axis=2).max(axis=0)
-        probe.close()
-        scn = _scaled(shell, 1.0 / float(np.median(peak)))  # maxima spread around threshold 1
-    eng = alg.EpochEngine.from_scenario(ctx, scn)
+@pytest.mark.parametrize("case", ["as_built", "front_truth", "front_model", "nan_voxel"])
+def test_final_metrics_match_oracle(alg, ctx, oracle_mod, shell, shell_front, case):
+    """States of the estimated model as built (maxima all near 1), of the ground-truth and estimated
+    models with the front part-way across, and of a model with one NaN voxel."""
+    scn = shell_front if case.startswith("front") else shell
+    eng = alg.EpochEngine.from_scenario(ctx, scn, truth=case == "front_truth")
     if case == "nan_voxel":
         g = scn.model.gains.copy()
         g[0:3] = np.nan
@@ -119,8 +119,8 @@ def test_final_metrics_match_oracle(alg, ctx, oracle_mod, shell, case):
         np.testing.assert_array_equal(getattr(got, f), want[f], err_msg=f)
     for f in ("threshold", "dice", "iou", "recall", "precision"):
         assert np.float32(getattr(got, f)) == np.float32(want[f]), f
-    if case == "maxima_spread_over_thresholds":
-        assert len(np.unique(want["dice_score_over_threshold"])) > 5  # the sweep is exercised
+    if case == "front_truth":
+        assert len(np.unique(want["dice_score_over_threshold"])) > 10  # the sweep is exercised
     eng.close()
 
 
