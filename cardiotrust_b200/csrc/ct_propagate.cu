@@ -72,39 +72,67 @@ __device__ __forceinline__ void named_arrive(int id, int count) {
   asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-// Stage one tile (all threads): metadata first (the gain mask needs it), then gains and chain state.
+// Stage one tile (all threads). Every global load of the tile (per-(voxel, offset) metadata, the
+// three gain rows, the chain state, the control column) is issued into registers before any of
+// them is stored, so the loads are in flight together (about 70 per thread) instead of one loop
+// iteration's worth at a time; the gain mask needs the staged neighbour table and is applied after
+// a barrier.
+constexpr int kStageItems = (kTileItems + kThreads - 1) / kThreads;
+constexpr int kStageCols = (kGainCols * kTileVoxels + kThreads - 1) / kThreads;
+static_assert(kTileStates <= kThreads, "one control entry per thread");
+
 __device__ __forceinline__ void stage_tile(Smem& sm, const FwdArgs& p, int v0) {
   const int nv = min(kTileVoxels, p.V - v0);
-  for (int e = threadIdx.x; e < kTileItems; e += blockDim.x) {
-    const int vl = e / kOffsets;
-    if (vl < nv) {
-      const int gi = v0 * kOffsets + e;
-      const int32_t nb = p.nbr[gi];
-      sm.j[e] = nb < 0 ? -1 : 3 * nb;
-      sm.d[e] = p.delays[gi];
-      sm.c[e] = p.coefs[gi];
-    } else {
-      sm.j[e] = -1;
-      sm.d[e] = 1;
-      sm.c[e] = 0.0f;
-    }
+  const int tid = threadIdx.x;
+  int32_t nb[kStageItems], dl[kStageItems];
+  float cf[kStageItems];
+  float gx[kStageCols], gy[kStageCols], gz[kStageCols], ap[kStageCols];
+#pragma unroll
+  for (int i = 0; i < kStageItems; ++i) {
+    const int e = tid + i * kThreads;
+    const bool ok = e < kTileItems && e / kOffsets < nv;
+    const int gi = v0 * kOffsets + (ok ? e : 0);
+    nb[i] = ok ? p.nbr[gi] : -1;
+    dl[i] = ok ? p.delays[gi] : 1;
+    cf[i] = ok ? p.coefs[gi] : 0.0f;
   }
-  for (int e = threadIdx.x; e < kTileStates; e += blockDim.x) sm.ctrl[e] = (e < 3 * nv) ? p.ctrl[3 * v0 + e] : 0.0f;
-  __syncthreads();
-  for (int e = threadIdx.x; e < kGainCols * kTileVoxels; e += blockDim.x) {
+#pragma unroll
+  for (int i = 0; i < kStageCols; ++i) {
+    const int e = tid + i * kThreads;
     const int k = e / kTileVoxels, vl = e - k * kTileVoxels;
-    float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (vl < nv && sm.j[vl * kOffsets + k / 3] >= 0) {
-      const float* row = p.gains + (size_t)3 * (v0 + vl) * kGainCols + k;
-      g.x = row[0];
-      g.y = row[kGainCols];
-      g.z = row[2 * kGainCols];
-    }
-    sm.g[k][vl] = g;
+    const bool ok = e < kGainCols * kTileVoxels && vl < nv;
+    const float* row = p.gains + (size_t)3 * (v0 + (ok ? vl : 0)) * kGainCols + (ok ? k : 0);
+    gx[i] = ok ? row[0] : 0.0f;
+    gy[i] = ok ? row[kGainCols] : 0.0f;
+    gz[i] = ok ? row[2 * kGainCols] : 0.0f;
+    ap[i] = (e < nv * kGainCols) ? p.ap[(size_t)v0 * kGainCols + e] : 0.0f;
   }
-  const float* a0 = p.ap + (size_t)v0 * kGainCols;
-  for (int e = threadIdx.x; e < kTileVoxels * kGainCols; e += blockDim.x)
-    sm.ap_state[e] = (e < nv * kGainCols) ? a0[e] : 0.0f;
+  const float ctl = (tid < 3 * nv) ? p.ctrl[3 * v0 + tid] : 0.0f;
+#pragma unroll
+  for (int i = 0; i < kStageItems; ++i) {
+    const int e = tid + i * kThreads;
+    if (e < kTileItems) {
+      sm.j[e] = nb[i] < 0 ? -1 : 3 * nb[i];
+      sm.d[e] = dl[i];
+      sm.c[e] = cf[i];
+    }
+  }
+  if (tid < kTileStates) sm.ctrl[tid] = ctl;
+#pragma unroll
+  for (int i = 0; i < kStageCols; ++i) {
+    const int e = tid + i * kThreads;
+    if (e < kTileVoxels * kGainCols) sm.ap_state[e] = ap[i];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kStageCols; ++i) {
+    const int e = tid + i * kThreads;
+    if (e < kGainCols * kTileVoxels) {
+      const int k = e / kTileVoxels, vl = e - k * kTileVoxels;
+      const bool live = sm.j[vl * kOffsets + k / 3] >= 0;  // absent neighbours add exact zeros
+      sm.g[k][vl] = live ? make_float4(gx[i], gy[i], gz[i], 0.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+  }
   __syncthreads();
 }
 
@@ -228,7 +256,7 @@ __device__ __forceinline__ void consume(Smem& sm, const FwdArgs& p, int v0, int 
   if (vl == 0) sm.part[r0 + s] = sm.part[r0 + s] + f2;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) forward_stream_kernel(FwdArgs p) {
+__global__ void __launch_bounds__(kThreads, 2) forward_stream_kernel(FwdArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
 
@@ -292,7 +320,7 @@ __global__ void __launch_bounds__(kThreads, 1) forward_stream_kernel(FwdArgs p) 
 // its own per-step max-regularisation partial, stepsum_part[t * part_stride +
 // tile of the scenario], so the step metrics of every scenario sum the same
 // partials in the same order.
-__global__ void __launch_bounds__(kThreads, 1) forward_batch_kernel(FwdBatch B) {
+__global__ void __launch_bounds__(kThreads, 2) forward_batch_kernel(FwdBatch B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   __shared__ FwdArgs sp;
