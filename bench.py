@@ -330,6 +330,68 @@ def post_run_section(alg, eng, scn, stream, hbm_peak, prec):
     }
 
 
+def _noisy_scenario(alg, sc, ctx, spec):
+    """A batch-workload scenario with its ground truth from the CUDA forward plus the spec's noise."""
+    import numpy as np
+
+    scn = sc.build(spec)
+    truth = alg.EpochEngine.from_scenario(ctx, scn, truth=True)
+    y = truth.simulate()
+    truth.close()
+    rng = np.random.default_rng(spec.seed + 7919)
+    sigma = spec.noise_fraction * float(np.sqrt(np.mean(y.astype(np.float64) ** 2)))
+    scn.measurements = (y + rng.normal(0.0, sigma, size=y.shape)).astype(np.float32)
+    return scn
+
+
+def batch_precision_check(alg, sc, ctx, specs, work, prec):
+    """Gradient error of the batched epoch's product precision on members of the batch workload, one
+    adjoint epoch from the initial parameters (beats in index order, as in the batch): the smallest,
+    median and largest members against the same epoch with FP32 products (which the precision report
+    places within ~1.5e-4 of the f64 oracle), and the smallest member with its beat cut to 600 steps
+    against the f64 oracle's adjoint gradient (the oracle needs ~20 s per 3,000-step beat of it)."""
+    import dataclasses
+
+    import numpy as np
+
+    import oracle
+
+    def rel(a, b):
+        b = np.asarray(b, np.float64)
+        return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+    cfg = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False,
+                        ap_derivative=alg.APDerivative.Textbook)
+
+    def gpu_grads(scn, precision):
+        eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=cfg)
+        eng.run_epoch(0, beat_order=np.arange(scn.num_beats), grad_mode=alg.GradMode.Adjoint, precision=precision)
+        g = (eng.read("grad_gains"), eng.read("grad_coefs"))
+        eng.close()
+        return g
+
+    def entry(i, scn, against, got, ref):
+        return {"member": int(i), "voxels": scn.num_voxels, "steps": scn.num_steps, "beats": scn.num_beats,
+                "states_multiple_of_4": scn.num_states % 4 == 0, "against": against,
+                "grad_gains": rel(got[0], ref[0]), "grad_coefs": rel(got[1], ref[1])}
+
+    order = np.argsort(work)
+    out = {"target": 1e-3, "members": []}
+    for i in (order[0], order[len(order) // 2], order[-1]):
+        scn = _noisy_scenario(alg, sc, ctx, specs[int(i)])
+        out["members"].append(entry(i, scn, "GPU epoch with FP32 products", gpu_grads(scn, prec),
+                                    gpu_grads(scn, alg.Precision.Fp32)))
+    i = order[0]
+    scn = _noisy_scenario(alg, sc, ctx, dataclasses.replace(specs[int(i)], num_steps=600))
+    o = oracle.from_scenario(scn, dtype=np.float64)
+    o.run_epoch(oracle.algo(optimizer=1, learning_rate=1e-3, freeze_delays=0, ap_derivative=1),
+                beat_order=np.arange(scn.num_beats, dtype=np.int32), adjoint=True)
+    out["members"].append(entry(i, scn, "f64 oracle adjoint (beat cut to 600 steps)", gpu_grads(scn, prec),
+                                (o.d_gains, o.d_coefs)))
+    out["max"] = max(max(m["grad_gains"], m["grad_coefs"]) for m in out["members"])
+    return out
+
+
 def batched_section(args, alg, sc, ctx, prec, stream, flush):
     """64 scenarios of uneven size (batch_workload_specs): the batched adjoint epoch (one forward and
     one adjoint launch per beat index over every member, replayed from a CUDA graph) against the plain
@@ -340,22 +402,16 @@ def batched_section(args, alg, sc, ctx, prec, stream, flush):
     specs = sc.batch_workload_specs(args.batch_scenarios, seed=0)
     cfg = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False,
                         ap_derivative=alg.APDerivative.Textbook)
-    engines, vtb, sizes = [], 0, []
-    slots = 2 + 5 + args.batch_epochs + 2  # warm-up, autotuner trials, timed epochs, plain epochs
+    engines, vtb, sizes, vtbs = [], 0, [], []
+    slots = 2 + 5 + args.batch_epochs + 1 + 2  # warm-up, autotuner trials, timed and profiled epochs, plain
     for sp in specs:
-        scn = sc.build(sp)
-        truth = alg.EpochEngine.from_scenario(ctx, scn, truth=True)
-        y = truth.simulate()
-        truth.close()
-        rng = np.random.default_rng(sp.seed + 7919)
-        sigma = sp.noise_fraction * float(np.sqrt(np.mean(y.astype(np.float64) ** 2)))
-        scn.measurements = (y + rng.normal(0.0, sigma, size=y.shape)).astype(np.float32)
+        scn = _noisy_scenario(alg, sc, ctx, sp)
         engines.append(alg.EpochEngine.from_scenario(ctx, scn, num_batch_slots=slots, algorithm=cfg))
         vtb += scn.num_voxels * scn.num_steps * scn.num_beats
+        vtbs.append(scn.num_voxels * scn.num_steps * scn.num_beats)
         sizes.append(scn.num_voxels)
         del scn
     build_s = time.perf_counter() - t0
-    n_tc = sum(1 for e in engines if e.dims["S"] % 4 == 0)
     batch = alg.EpochBatch(ctx, engines, grad_mode=alg.GradMode.Adjoint, precision=prec)
     batch.run_epoch(sync=True)  # warm-up: captures the epoch graph
     tuned = batch.autotune()    # up to five trial epochs (they train); keeps the fastest schedule
@@ -363,6 +419,11 @@ def batched_section(args, alg, sc, ctx, prec, stream, flush):
     ms = timed_epochs(stream, lambda: batch.run_epoch(sync=False), args.batch_epochs, flush)
     batch.sync()
     info = batch.info()
+    # one more epoch as eager launches with CUDA events around each phase (where the epoch goes)
+    batch.set_profiling(True)
+    batch.run_epoch(sync=True)
+    phases = {k: v for k, v in batch.read_profile().items() if v > 0}
+    batch.set_profiling(False)
     chosen_ms = statistics.mean(ms)
     n = len(engines)
     # plain one-scenario form over every member, one epoch each (after one warm-up epoch of the smallest)
@@ -374,6 +435,7 @@ def batched_section(args, alg, sc, ctx, prec, stream, flush):
     batch.close()
     for e in engines:
         e.close()
+    check = batch_precision_check(alg, sc, ctx, specs, vtbs, prec)
     chosen = n * 1000.0 / chosen_ms
     plain = n * 1000.0 / plain_ms
     return {
@@ -383,16 +445,17 @@ def batched_section(args, alg, sc, ctx, prec, stream, flush):
         "scenarios": n, "voxels_total": int(sum(sizes)), "voxel_steps_per_epoch": int(vtb),
         "build_s": build_s,
         "chosen": {"form": "batched: one persistent forward and one persistent adjoint launch per beat index over "
-                           "every member's tiles, epoch replayed from a CUDA graph; adjoint gradients, checkpoints "
-                           "every 64 steps", "precision": f"{['fp32', 'tf32x3', 'tf32'][int(prec)]} products for the {n_tc} members "
-                                         "whose state count is a multiple of 4, fp32 for the others",
+                           "every member's tiles, epoch replayed from a CUDA graph; adjoint gradients, checkpoint interval "
+                           "from the autotuner", "precision": f"{['fp32', 'tf32x3', 'tf32'][int(prec)]} products for every member",
                    "scenario_epochs_per_s": chosen, "voxel_steps_per_s": vtb * 1000.0 / chosen_ms,
                    "ms_per_epoch": chosen_ms, "graph_kernels": info["graph_kernels"], "uses_graph": info["uses_graph"],
-                   "forward_ctas": info["forward_ctas"], "adjoint_ctas": info["adjoint_ctas"], "autotuned": tuned},
+                   "forward_ctas": info["forward_ctas"], "adjoint_ctas": info["adjoint_ctas"], "autotuned": tuned,
+                   "eager_phase_ms": phases},
         "plain": {"form": "plain GPU form, one scenario at a time, one launch per phase per step (reference "
                           "gradients, FP32)", "scenario_epochs_per_s": plain,
                   "voxel_steps_per_s": vtb * 1000.0 / plain_ms, "ms_per_epoch_all": plain_ms},
         "chosen_vs_plain": chosen / plain,
+        "gradient_error": check,
     }
 
 

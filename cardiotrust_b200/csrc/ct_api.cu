@@ -797,7 +797,8 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
     ks = std::min<int64_t>(ks, std::max<int64_t>(1, S / 256));
     d.ksplit = (int)std::max<int64_t>(1, std::min<int64_t>(ks, 64));
   }
-  d.umma = ct::umma_supported(S, M);
+  d.umma = ct::umma_supported(M);
+  d.spad = (S + 3) / 4 * 4;
   d.kpad = ((M + 31) / 32) * 32;
   d.ksplit_umma = d.umma ? ct::umma_ksplit(T, S, M, ctx->num_sms) : 1;
   const int64_t V = d.V, mpad = ((M + 63) / 64) * 64;
@@ -848,8 +849,9 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   ALLOC(d.stepsum_part, T * d.fwd_grid);
   ALLOC(d.gemm_part, part_floats);
   if (d.umma) {
-    ALLOC(d.H_hi, B * M * S);
-    ALLOC(d.H_lo, B * M * S);
+    ALLOC(d.H_hi, B * M * d.spad);
+    ALLOC(d.H_lo, B * M * d.spad);
+    if (d.spad != S) ALLOC(d.Xpad, T * d.spad);
     ALLOC(d.Ht_hi, B * S * d.kpad);
     ALLOC(d.Ht_lo, B * S * d.kpad);
     ALLOC(d.R_hi, T * d.kpad);
@@ -1004,7 +1006,7 @@ static int run_epoch_impl(ct_scn* scn, int64_t* batch_index, const int32_t* beat
     return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
   if (precision != CT_PREC_FP32 && !scn->d.umma)
     return fail(CT_ERR_NOT_SUPPORTED,
-                "tensor-core precision needs num_states divisible by 4 (16-byte TMA rows) and the driver's TMA encoder");
+                "tensor-core precision needs the driver's TMA encoder and at most 65,536 sensor rows");
   CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
   DeviceScenario& d = scn->d;
   const ct_algorithm& a = scn->algo;

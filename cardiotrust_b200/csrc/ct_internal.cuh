@@ -62,7 +62,9 @@ struct DeviceScenario {
   bool umma;             // S % 4 == 0 and the TMA encoder is available
   int ksplit_umma;       // split-K factor of the tensor-core H x
   int64_t kpad;          // M rounded up to 32 (K extent of H^T r)
-  float* H_hi, *H_lo;    // [B,M,S] TF32 split of H
+  int64_t spad;          // S rounded up to 4: row pitch of H_hi, H_lo and Xpad (16-byte TMA rows)
+  float* H_hi, *H_lo;    // [B,M,spad] TF32 split of H, zero beyond S
+  float* Xpad;           // [T,spad] copy of X for the H x operand when S % 4 != 0 (else null)
   float* Ht_hi, *Ht_lo;  // [B,S,kpad] TF32 split of H^T, zero padded
   float* R_hi, *R_lo;    // [T,kpad] TF32 split of the residuals
   int32_t* dmin;         // [2] smallest and largest delay of a connected (voxel, offset) pair
@@ -145,7 +147,7 @@ cudaError_t launch_map_residuals(DeviceScenario& d, int64_t beat, cudaStream_t s
 cudaError_t launch_mse(DeviceScenario& d, cudaStream_t stream);
 
 // Tensor-core (tcgen05) forms, ct_umma.cu.
-bool umma_supported(int64_t S, int64_t M);
+bool umma_supported(int64_t M);
 int umma_yn(int64_t M);
 int umma_ksplit(int64_t T, int64_t S, int64_t M, int sms);
 cudaError_t umma_prepare(DeviceScenario& d, cudaStream_t stream);

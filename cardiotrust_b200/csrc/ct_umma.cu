@@ -387,14 +387,27 @@ __global__ void __launch_bounds__(kThreadsUmma, 1)
 
 // ---- operand preparation kernels
 
+// hi/lo [rows, pitch] = split(src [rows, cols]), zero in the columns cols..pitch-1.
 __global__ void split_tf32_kernel(const float* __restrict__ src, float* __restrict__ hi, float* __restrict__ lo,
-                                  long long n) {
+                                  long long rows, int cols, int pitch) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float v = src[i];
+  if (i >= rows * pitch) return;
+  const long long r = i / pitch;
+  const int c = (int)(i - r * pitch);
+  const float v = c < cols ? src[r * cols + c] : 0.0f;
   const float h = tf32_rna(v);
   hi[i] = h;
   lo[i] = tf32_rna(v - h);
+}
+
+// dst [rows, pitch] = src [rows, cols], zero in the columns cols..pitch-1 (16-byte TMA rows).
+__global__ void pad_rows_kernel(const float* __restrict__ src, float* __restrict__ dst, long long rows, int cols,
+                                int pitch) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * pitch) return;
+  const long long r = i / pitch;
+  const int c = (int)(i - r * pitch);
+  dst[i] = c < cols ? src[r * cols + c] : 0.0f;
 }
 
 // Ht[b][s][k] = split(H[b][k][s]) for k < M, zero for M <= k < kpad.
@@ -502,8 +515,10 @@ cudaError_t launch_gemm(const CUtensorMap& a, const CUtensorMap& a_lo, const CUt
 
 // ---- public launchers (ct_internal.cuh)
 
-// Rows of X and H^T need 16-byte strides (S % 4 == 0); sensor rows beyond 256 take more column tiles of H x.
-bool umma_supported(int64_t S, int64_t M) { return (S % 4) == 0 && M <= 65536 && encode_fn() != nullptr; }
+// Sensor rows beyond 256 take more column tiles of H x. Any state count: the K-major operands of H x
+// need 16-byte rows, so H's split is stored with a pitch of S rounded up to 4 and, when S % 4 != 0,
+// X is copied into a padded buffer before the product (the zero columns add exact zeros).
+bool umma_supported(int64_t M) { return M <= 65536 && encode_fn() != nullptr; }
 
 int umma_yn(int64_t M) { return M <= 128 ? 128 : 256; }
 
@@ -517,8 +532,9 @@ int umma_ksplit(int64_t T, int64_t S, int64_t M, int sms) {
 }
 
 cudaError_t umma_prepare(DeviceScenario& d, cudaStream_t stream) {
-  const long long n = (long long)d.B * d.M * d.S;
-  split_tf32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(d.H, d.H_hi, d.H_lo, n);
+  const long long n = (long long)d.B * d.M * d.spad;
+  split_tf32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(d.H, d.H_hi, d.H_lo, (long long)d.B * d.M,
+                                                                      (int)d.S, (int)d.spad);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((d.S + 31) / 32), (unsigned)(d.kpad / 32), (unsigned)d.B);
@@ -528,12 +544,20 @@ cudaError_t umma_prepare(DeviceScenario& d, cudaStream_t stream) {
 
 cudaError_t launch_measure_umma(DeviceScenario& d, int64_t beat, bool with_residuals, int precision,
                                 cudaStream_t stream) {
-  const int T = (int)d.T, S = (int)d.S, M = (int)d.M;
+  const int T = (int)d.T, S = (int)d.spad, M = (int)d.M;
   CUtensorMap mx, mh, mhl;
   const int yn = umma_yn(M);
-  const float* Hh = d.H_hi + beat * d.M * d.S;
-  const float* Hl = d.H_lo + beat * d.M * d.S;
-  if (!make_map(&mx, d.X, S, T, kBM) || !make_map(&mh, Hh, S, M, yn) || !make_map(&mhl, Hl, S, M, yn))
+  const float* Hh = d.H_hi + beat * d.M * d.spad;
+  const float* Hl = d.H_lo + beat * d.M * d.spad;
+  const float* X = d.X;
+  if (d.spad != d.S) {
+    const long long n = (long long)T * d.spad;
+    pad_rows_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(d.X, d.Xpad, T, (int)d.S, (int)d.spad);
+    cudaError_t e0 = cudaGetLastError();
+    if (e0 != cudaSuccess) return e0;
+    X = d.Xpad;
+  }
+  if (!make_map(&mx, X, S, T, kBM) || !make_map(&mh, Hh, S, M, yn) || !make_map(&mhl, Hl, S, M, yn))
     return cudaErrorInvalidValue;
   const int kchunks = (S + kBK - 1) / kBK;
   const int ldp = ((M + yn - 1) / yn) * yn;

@@ -202,8 +202,7 @@ int ct_run_epoch_plain(ct_scn* scn, int64_t* batch_index, const int32_t* beat_or
  * reference derivations, then every member's update. The epoch is captured once as a CUDA
  * graph and replayed (re-captured when a member's algorithm or adjoint ring changes).
  * Members need batch_size 0 (one update per epoch, the reference default) and the same
- * context; their beats run in index order. With a tensor-core precision, members whose
- * num_states is not a multiple of 4 use the FP32 products. Results equal ct_run_epoch with beat_order
+ * context; their beats run in index order. Results equal ct_run_epoch with beat_order
  * 0..B-1 within the tolerances of the measurement products. The members stay usable on
  * their own; a batch must be destroyed before its members. */
 typedef struct ct_batch ct_batch;

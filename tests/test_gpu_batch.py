@@ -84,13 +84,14 @@ def test_batch_matches_single_runs(alg, ctx, members, mode):
 
 
 def test_batch_tensor_core_precision(alg, ctx, members):
+    """Every member on the tensor cores, including those whose state count is not a multiple of 4."""
     algo = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
-    usable = [m for m in members if m.num_states % 4 == 0]
-    batched = _engines(alg, ctx, usable, algo)
-    single = _engines(alg, ctx, usable, algo)
+    assert any(m.num_states % 4 for m in members)
+    batched = _engines(alg, ctx, members, algo)
+    single = _engines(alg, ctx, members, algo)
     batch = alg.EpochBatch(ctx, batched, grad_mode=alg.GradMode.Adjoint, precision=alg.Precision.Tf32x3)
     batch.run_epoch()
-    for m, e in zip(usable, single):
+    for m, e in zip(members, single):
         e.run_epoch(0, beat_order=np.arange(m.num_beats), grad_mode=alg.GradMode.Adjoint,
                     precision=alg.Precision.Tf32x3)
     for b, e in zip(batched, single):

@@ -352,6 +352,30 @@ def test_tensor_core_many_sensor_rows(alg, ctx, oracle_mod):
         eng.close()
 
 
+@pytest.mark.parametrize("shape", [(5, 5, 5), (7, 3, 3), (6, 5, 3)])
+def test_tensor_core_state_count_not_multiple_of_4(alg, ctx, oracle_mod, shape):
+    """States not a multiple of 4 (375, 189 and 270 states): the H x operand is padded to 16-byte rows
+    (zero columns) and the tcgen05 products keep the FP32 bars, in both gradient modes."""
+    from cardiotrust_b200 import scenario as sc
+
+    spec = sc.ScenarioSpec(shape=shape, num_steps=160, num_sensors=20, patho_size=2, patho_origin=(1, 1, 1),
+                           pulse_onset=1, pulse_sigma_samples=4.0, noise_fraction=0.01, seed=13)
+    scn = sc.attach_measurements(sc.build(spec), oracle_forward(oracle_mod))
+    assert scn.num_states % 4 != 0
+    a, oa = algo_pair(alg, oracle_mod, optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
+    o64 = oracle_mod.from_scenario(scn, dtype=np.float64)
+    o64.run_epoch(oa)
+    adj = oracle_mod.from_scenario(scn, dtype=np.float64)
+    adj.run_epoch(oa, adjoint=True)
+    for mode, ref in ((alg.GradMode.Reference, o64), (alg.GradMode.Adjoint, adj)):
+        eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=a)
+        eng.run_epoch(0, grad_mode=mode, precision=alg.Precision.Tf32x3)
+        assert rel_err(eng.read("measurements"), ref.measurements) < TOL_MEAS, mode
+        assert rel_err(eng.read("grad_gains"), ref.d_gains) < TOL_GRAD, mode
+        assert rel_err(eng.read("grad_coefs"), ref.d_coefs) < TOL_GRAD, mode
+        eng.close()
+
+
 def _mr_history(o64, scn):
     """H^T r of every step of the last beat, in float64, from the oracle's residuals."""
     H = scn.measurement_matrix[-1].astype(np.float64)
