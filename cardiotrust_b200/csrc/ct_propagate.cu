@@ -18,21 +18,26 @@
 //   * The all-pass state is deduplicated: ap_outputs[3v+a, 3n+b] does not
 //     depend on the row component a (same input state, coefficient and zero
 //     start, prediction.rs:56-79), so it is kept as [V, 26*3].
-//   * Warp specialisation. A block of L steps runs as rounds of kRound steps
-//     through a double-buffered ring of all-pass outputs in shared memory.
-//     Producer warps: one thread per (voxel, offset) runs the three all-pass
-//     chains of the round; its 3 (kRound + 1) history loads are independent.
-//     Consumer warps: one thread per (voxel, step) accumulates the three rows
-//     x[t, 3v+a] over the 78 columns in order k = 0..77 (float2 all-pass and
-//     float4 gain loads feed three independent chains), adds the control
-//     input, stores the states and the voxel's max-regularisation term.
-//     Named barriers hand the two buffers back and forth; no CTA-wide barrier
-//     separates the roles inside a block.
-//   * Shared memory per tile: gains as float4 {g[3v][k], g[3v+1][k],
-//     g[3v+2][k], 0} (absent neighbours zeroed, which adds exact zeros where
-//     the reference skips), (neighbour, delay, coefficient) per (voxel,
-//     offset), the chain state, and the two round buffers. A CTA that owns one
-//     tile stages it once per launch.
+//   * Resident form (forward_ring_kernel): warp specialisation. A block of L
+//     steps runs as rounds of kRound steps through a double-buffered ring of
+//     all-pass outputs in shared memory. Producer warps: one thread per
+//     (voxel, offset) runs the three all-pass chains of the round; its
+//     3 (kRound + 1) history loads are independent. Consumer warps: one thread
+//     per (voxel, step) accumulates the three rows x[t, 3v+a] over the 78
+//     columns in order k = 0..77, adds the control input, stores the states
+//     and the voxel's max-regularisation term. Named barriers hand the two
+//     buffers back and forth.
+//   * Streaming forms (forward_stream_kernel, forward_batch_kernel): every
+//     thread takes both roles in turn, separated by CTA barriers: producer of
+//     4-5 (voxel, offset) items, then consumer of one (step, row, voxel) state
+//     (one accumulation chain over k = 0..77 per thread, three times the
+//     consumer threads of the resident form). During the consumer phase each
+//     thread already has the next round's history loads in flight, or in a
+//     visit's last round the next tile's staging loads.
+//   * Shared memory per tile: gains (absent neighbours zeroed, which adds
+//     exact zeros where the reference skips), (neighbour, delay, coefficient)
+//     per (voxel, offset), the chain state, and the round buffers. A CTA that
+//     owns one tile stages it once per launch.
 //   * History reads go through L1: within one launch a history row is read
 //     only after the grid barrier that completes it, so no SM can hold a
 //     stale line of it (L1 holds no global data across launches).
@@ -51,17 +56,28 @@ constexpr int kRound = 2;                            // steps per round
 constexpr int kProducers = 128;                      // 4 warps
 constexpr int kConsumers = kRound * kTileVoxels;     // 2 warps: (step, voxel)
 constexpr int kThreads = kProducers + kConsumers;
-constexpr int kBarFull = 1;   // named barriers kBarFull + buffer, kBarEmpty + buffer
+constexpr int kBarFull = 1;   // named barriers kBarFull + buffer, kBarEmpty + buffer (resident form)
 constexpr int kBarEmpty = 3;
+constexpr int kItemsPerProducer = (kTileItems + kProducers - 1) / kProducers;  // resident form
+
+// Streaming forms (a CTA walks several tiles, re-staging each per block of steps). All 192 threads
+// take both roles in turn: producers, one thread per (voxel, offset) item (4-5 items each), then
+// consumers, one thread per (step, row a, voxel) state of the round; CTA barriers separate the two.
+// While the consumers work, each thread already holds the next round's history loads (or, in a
+// visit's last round, the next tile's staging loads) in flight.
+constexpr int kApPitch = kGainCols + 1;  // odd row pitch of the round buffer: conflict-free reads
+constexpr int kLsItems = (kTileItems + kThreads - 1) / kThreads;
+static_assert(kRound * 3 * kTileVoxels == kThreads, "one consumer thread per (step, row, voxel)");
 
 struct Smem {
-  float4 g[kGainCols][kTileVoxels];                  // gains of the voxel's three rows at column k
-  float ap_out[2][kRound][kTileVoxels * kGainCols];  // round buffers
+  float g[3][kGainCols][kTileVoxels];             // gain g[3v+a][k] at [a][k][v] (absent neighbours zero)
+  float ap_out[kRound][kTileVoxels * kApPitch];   // all-pass outputs of the round's steps
   float ap_state[kTileVoxels * kGainCols];
-  int32_t j[kTileItems];                             // 3 * neighbour, -1 if absent
+  int32_t j[kTileItems];                          // 3 * neighbour, -1 if absent
   int32_t d[kTileItems];
   float c[kTileItems];
   float ctrl[kTileStates];
+  float xs[kRound][3][kTileVoxels];               // the round's states, for the regularisation term
   float part[kMaxStepBlock];
 };
 
@@ -72,29 +88,32 @@ __device__ __forceinline__ void named_arrive(int id, int count) {
   asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-// Stage one tile (all threads). Every global load of the tile (per-(voxel, offset) metadata, the
-// three gain rows, the chain state, the control column) is issued into registers before any of
-// them is stored, so the loads are in flight together (about 70 per thread) instead of one loop
-// iteration's worth at a time; the gain mask needs the staged neighbour table and is applied after
-// a barrier.
+// A tile's staging loads, held in registers between their issue and their store to shared
+// memory, so that they can be issued before the previous tile's visit ends.
 constexpr int kStageItems = (kTileItems + kThreads - 1) / kThreads;
 constexpr int kStageCols = (kGainCols * kTileVoxels + kThreads - 1) / kThreads;
 static_assert(kTileStates <= kThreads, "one control entry per thread");
 
-__device__ __forceinline__ void stage_tile(Smem& sm, const FwdArgs& p, int v0) {
-  const int nv = min(kTileVoxels, p.V - v0);
-  const int tid = threadIdx.x;
+struct StageRegs {
   int32_t nb[kStageItems], dl[kStageItems];
   float cf[kStageItems];
   float gx[kStageCols], gy[kStageCols], gz[kStageCols], ap[kStageCols];
+  float ctl;
+};
+
+// Issue every global load of tile v0 of scenario p (metadata, the three gain rows, chain state,
+// control column) into registers; nothing waits for them here.
+__device__ __forceinline__ void stage_load(StageRegs& r, const FwdArgs& p, int v0) {
+  const int nv = min(kTileVoxels, p.V - v0);
+  const int tid = threadIdx.x;
 #pragma unroll
   for (int i = 0; i < kStageItems; ++i) {
     const int e = tid + i * kThreads;
     const bool ok = e < kTileItems && e / kOffsets < nv;
     const int gi = v0 * kOffsets + (ok ? e : 0);
-    nb[i] = ok ? p.nbr[gi] : -1;
-    dl[i] = ok ? p.delays[gi] : 1;
-    cf[i] = ok ? p.coefs[gi] : 0.0f;
+    r.nb[i] = ok ? p.nbr[gi] : -1;
+    r.dl[i] = ok ? p.delays[gi] : 1;
+    r.cf[i] = ok ? p.coefs[gi] : 0.0f;
   }
 #pragma unroll
   for (int i = 0; i < kStageCols; ++i) {
@@ -102,26 +121,32 @@ __device__ __forceinline__ void stage_tile(Smem& sm, const FwdArgs& p, int v0) {
     const int k = e / kTileVoxels, vl = e - k * kTileVoxels;
     const bool ok = e < kGainCols * kTileVoxels && vl < nv;
     const float* row = p.gains + (size_t)3 * (v0 + (ok ? vl : 0)) * kGainCols + (ok ? k : 0);
-    gx[i] = ok ? row[0] : 0.0f;
-    gy[i] = ok ? row[kGainCols] : 0.0f;
-    gz[i] = ok ? row[2 * kGainCols] : 0.0f;
-    ap[i] = (e < nv * kGainCols) ? p.ap[(size_t)v0 * kGainCols + e] : 0.0f;
+    r.gx[i] = ok ? row[0] : 0.0f;
+    r.gy[i] = ok ? row[kGainCols] : 0.0f;
+    r.gz[i] = ok ? row[2 * kGainCols] : 0.0f;
+    r.ap[i] = (e < nv * kGainCols) ? p.ap[(size_t)v0 * kGainCols + e] : 0.0f;
   }
-  const float ctl = (tid < 3 * nv) ? p.ctrl[3 * v0 + tid] : 0.0f;
+  r.ctl = (tid < 3 * nv) ? p.ctrl[3 * v0 + tid] : 0.0f;
+}
+
+// Store staged registers to shared memory (all threads, after every read of the previous tile's
+// shared data); the gain mask needs the neighbour table and is applied after a barrier.
+__device__ __forceinline__ void stage_store(Smem& sm, const StageRegs& r) {
+  const int tid = threadIdx.x;
 #pragma unroll
   for (int i = 0; i < kStageItems; ++i) {
     const int e = tid + i * kThreads;
     if (e < kTileItems) {
-      sm.j[e] = nb[i] < 0 ? -1 : 3 * nb[i];
-      sm.d[e] = dl[i];
-      sm.c[e] = cf[i];
+      sm.j[e] = r.nb[i] < 0 ? -1 : 3 * r.nb[i];
+      sm.d[e] = r.dl[i];
+      sm.c[e] = r.cf[i];
     }
   }
-  if (tid < kTileStates) sm.ctrl[tid] = ctl;
+  if (tid < kTileStates) sm.ctrl[tid] = r.ctl;
 #pragma unroll
   for (int i = 0; i < kStageCols; ++i) {
     const int e = tid + i * kThreads;
-    if (e < kTileVoxels * kGainCols) sm.ap_state[e] = ap[i];
+    if (e < kTileVoxels * kGainCols) sm.ap_state[e] = r.ap[i];
   }
   __syncthreads();
 #pragma unroll
@@ -130,7 +155,9 @@ __device__ __forceinline__ void stage_tile(Smem& sm, const FwdArgs& p, int v0) {
     if (e < kGainCols * kTileVoxels) {
       const int k = e / kTileVoxels, vl = e - k * kTileVoxels;
       const bool live = sm.j[vl * kOffsets + k / 3] >= 0;  // absent neighbours add exact zeros
-      sm.g[k][vl] = live ? make_float4(gx[i], gy[i], gz[i], 0.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      sm.g[0][k][vl] = live ? r.gx[i] : 0.0f;
+      sm.g[1][k][vl] = live ? r.gy[i] : 0.0f;
+      sm.g[2][k][vl] = live ? r.gz[i] : 0.0f;
     }
   }
   __syncthreads();
@@ -142,18 +169,14 @@ __device__ __forceinline__ void unstage_tile(Smem& sm, const FwdArgs& p, int v0)
   for (int e = threadIdx.x; e < nv * kGainCols; e += blockDim.x) a0[e] = sm.ap_state[e];
 }
 
-// Producer: all-pass chains of steps tr0 .. tr0+R-1 into round buffer `buf`. Each thread owns
-// up to kItemsPerProducer (voxel, offset) items and issues the history loads of all of them
-// before any chain arithmetic, so ~60 independent loads are in flight per thread.
-constexpr int kItemsPerProducer = (kTileItems + kProducers - 1) / kProducers;
-
-__device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int nv, int tr0, int R, int buf) {
-  // h[i][q][b] = x[tr0 - d_i - 1 + q, j_i + b]: in(tr0+s) = h[s+1], in_delayed(tr0+s) = h[s];
-  // rows before t = 0 read as zero (prediction.rs:68-77)
-  float h[kItemsPerProducer][kRound + 1][3];
+// History of the thread's items for the round starting at tr0: h[i][q][b] = x[tr0 - d_i - 1 + q,
+// j_i + b] (rows before t = 0 read as zero, prediction.rs:68-77). Every row read within a block of
+// L <= dmin steps is older than the block, so these loads may be issued at any time in the block.
+__device__ __forceinline__ void load_history(float (&h)[kLsItems][kRound + 1][3], const Smem& sm, const FwdArgs& p,
+                                             int tr0, int R) {
 #pragma unroll
-  for (int i = 0; i < kItemsPerProducer; ++i) {
-    const int e = threadIdx.x + i * kProducers;
+  for (int i = 0; i < kLsItems; ++i) {
+    const int e = threadIdx.x + i * kThreads;
     const int jb = e < kTileItems ? sm.j[e] : -1;
     const int d = e < kTileItems ? sm.d[e] : 0;
 #pragma unroll
@@ -165,6 +188,11 @@ __device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int 
       for (int b = 0; b < 3; ++b) h[i][q][b] = ok ? row[b] : 0.0f;
     }
   }
+}
+
+// Producer: all-pass chains of the thread's items for steps tr0 .. tr0+R-1 into the round buffer.
+__device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int nv, int tr0, int R,
+                                        const float (&h)[kLsItems][kRound + 1][3]) {
   // adjoint checkpoint inside this round: step index after which the state is stored, or -1
   int ck_s = -1;
   float* ck_row = nullptr;
@@ -176,14 +204,14 @@ __device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int 
     }
   }
 #pragma unroll
-  for (int i = 0; i < kItemsPerProducer; ++i) {
-    const int e = threadIdx.x + i * kProducers;
+  for (int i = 0; i < kLsItems; ++i) {
+    const int e = threadIdx.x + i * kThreads;
     if (e >= kTileItems) break;
     const int vl = e / kOffsets;
     const int n = e - vl * kOffsets;
     const int jb = sm.j[e];
     float* st = sm.ap_state + vl * kGainCols + 3 * n;
-    float* out0 = sm.ap_out[buf][0] + vl * kGainCols + 3 * n;
+    float* out0 = sm.ap_out[0] + vl * kApPitch + 3 * n;
     if (jb >= 0) {
       const float c = sm.c[e];
 #pragma unroll
@@ -193,7 +221,7 @@ __device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int 
         for (int s = 0; s < kRound; ++s) {
           if (s < R) {
             a = fmaf(c, h[i][s + 1][b] - a, h[i][s][b]);
-            out0[s * (kTileVoxels * kGainCols) + b] = a;
+            out0[s * (kTileVoxels * kApPitch) + b] = a;
             if (tr0 + s == p.T - 2) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = a;
             if (s == ck_s) ck_row[vl * kGainCols + 3 * n + b] = a;
           }
@@ -205,7 +233,7 @@ __device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int 
       for (int s = 0; s < kRound; ++s)
         if (s < R)
 #pragma unroll
-          for (int b = 0; b < 3; ++b) out0[s * (kTileVoxels * kGainCols) + b] = 0.0f;
+          for (int b = 0; b < 3; ++b) out0[s * (kTileVoxels * kApPitch) + b] = 0.0f;
       if (vl < nv && p.T - 2 >= tr0 && p.T - 2 < tr0 + R)
 #pragma unroll
         for (int b = 0; b < 3; ++b) p.ap_last[(size_t)(v0 + vl) * kGainCols + 3 * n + b] = st[b];
@@ -213,39 +241,34 @@ __device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int 
   }
 }
 
-// Consumer: states of step tr0 + s for voxel vl (thread = (s, vl)), and the voxel's
-// max-regularisation term reduced over the warp (the warp covers one step).
-__device__ __forceinline__ void consume(Smem& sm, const FwdArgs& p, int v0, int nv, int tr0, int R, int buf,
-                                       int r0) {
-  const int ct = threadIdx.x - kProducers;
-  const int s = ct / kTileVoxels, vl = ct - s * kTileVoxels;
-  if (s >= R) return;  // warp-uniform
+// Consumer: the state x[tr0 + s, 3 (v0 + vl) + a] (thread = (s, a, vl)), accumulated over the 78
+// columns in the reference's order, plus the control input; stored to X and to the round's xs.
+__device__ __forceinline__ void consume(Smem& sm, const FwdArgs& p, int v0, int nv, int tr0, int R) {
+  const int s = threadIdx.x / (3 * kTileVoxels);
+  const int a = (threadIdx.x / kTileVoxels) % 3;
+  const int vl = threadIdx.x % kTileVoxels;
+  if (s >= R || vl >= nv) return;
+  const float* aps = sm.ap_out[s] + vl * kApPitch;
+  const float* gs = &sm.g[a][0][vl];
+  float x = 0.0f;
+#pragma unroll 13
+  for (int k = 0; k < kGainCols; ++k) x = x + gs[k * kTileVoxels] * aps[k];
+  const int t = tr0 + s;
+  x = x + p.u[t] * sm.ctrl[3 * vl + a];
+  p.X[(size_t)t * p.S + 3 * (v0 + vl) + a] = x;
+  sm.xs[s][a][vl] = x;
+}
+
+// The voxels' max-regularisation terms of the round's step s (warp s * 3 of the consumers, lane =
+// voxel), reduced over the warp in lane order and added to part[r0 + s].
+__device__ __forceinline__ void regularise(Smem& sm, const FwdArgs& p, int nv, int R, int r0) {
+  const int s = threadIdx.x / (3 * kTileVoxels);
+  const int a = (threadIdx.x / kTileVoxels) % 3;
+  const int vl = threadIdx.x % kTileVoxels;
+  if (a != 0 || s >= R) return;  // warp-uniform
   float f2 = 0.0f;
   if (vl < nv) {
-    const float* aps = sm.ap_out[buf][s] + vl * kGainCols;
-    float x0 = 0.0f, x1 = 0.0f, x2 = 0.0f;
-#pragma unroll 3
-    for (int k = 0; k < kGainCols; k += 2) {
-      const float2 a = *reinterpret_cast<const float2*>(aps + k);
-      const float4 g0 = sm.g[k][vl];
-      const float4 g1 = sm.g[k + 1][vl];
-      x0 = x0 + g0.x * a.x;
-      x1 = x1 + g0.y * a.x;
-      x2 = x2 + g0.z * a.x;
-      x0 = x0 + g1.x * a.y;
-      x1 = x1 + g1.y * a.y;
-      x2 = x2 + g1.z * a.y;
-    }
-    const int t = tr0 + s;
-    const float uc = p.u[t];
-    x0 = x0 + uc * sm.ctrl[3 * vl];
-    x1 = x1 + uc * sm.ctrl[3 * vl + 1];
-    x2 = x2 + uc * sm.ctrl[3 * vl + 2];
-    float* xo = p.X + (size_t)t * p.S + 3 * (v0 + vl);
-    xo[0] = x0;
-    xo[1] = x1;
-    xo[2] = x2;
-    const float sum = fabsf(x0) + fabsf(x1) + fabsf(x2);
+    const float sum = fabsf(sm.xs[s][0][vl]) + fabsf(sm.xs[s][1][vl]) + fabsf(sm.xs[s][2][vl]);
     if (sum > p.threshold) {
       const float f = sum - p.threshold;
       f2 = f * f;
@@ -256,6 +279,28 @@ __device__ __forceinline__ void consume(Smem& sm, const FwdArgs& p, int v0, int 
   if (vl == 0) sm.part[r0 + s] = sm.part[r0 + s] + f2;
 }
 
+// One visit of a tile: L steps from t0 in rounds of kRound. `h` holds the first round's history on
+// entry; with `next` set, the last round's consumer phase also issues the next tile's staging loads
+// into `nx` (stored by the caller after this visit).
+__device__ __forceinline__ void visit_tile(Smem& sm, const FwdArgs& p, int v0, int nv, int t0, int L,
+                                           float (&h)[kLsItems][kRound + 1][3], const FwdArgs* next, int next_v0,
+                                           StageRegs& nx) {
+  for (int r0 = 0; r0 < L; r0 += kRound) {
+    const int R = (L - r0) < kRound ? (L - r0) : kRound;
+    produce(sm, p, v0, nv, t0 + r0, R, h);
+    __syncthreads();
+    if (r0 + kRound < L) {
+      const int Rn = (L - r0 - kRound) < kRound ? (L - r0 - kRound) : kRound;
+      load_history(h, sm, p, t0 + r0 + kRound, Rn);
+    } else if (next) {
+      stage_load(nx, *next, next_v0);
+    }
+    consume(sm, p, v0, nv, t0 + r0, R);
+    __syncthreads();
+    regularise(sm, p, nv, R, r0);
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 2) forward_stream_kernel(FwdArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
@@ -263,40 +308,41 @@ __global__ void __launch_bounds__(kThreads, 2) forward_stream_kernel(FwdArgs p) 
   const int V = p.V, T = p.T;
   const int num_tiles = (V + kTileVoxels - 1) / kTileVoxels;
   const bool resident = num_tiles <= (int)gridDim.x;  // this CTA owns at most one tile
-  const bool producer = threadIdx.x < kProducers;
   int dmin = p.dmin[0];
   if (dmin < 1) dmin = 1;
   const int Lmax = dmin < kMaxStepBlock ? dmin : kMaxStepBlock;
+  float h[kLsItems][kRound + 1][3];
+  StageRegs nx;
 
-  if (resident && (int)blockIdx.x < num_tiles) stage_tile(sm, p, blockIdx.x * kTileVoxels);
-
-  int round = 0;  // rounds issued by this CTA, pairs the named barriers across blocks and tiles
+  if (resident && (int)blockIdx.x < num_tiles) {
+    stage_load(nx, p, blockIdx.x * kTileVoxels);
+    stage_store(sm, nx);
+  }
   unsigned int barrier_number = 0;
   for (int t0 = 0; t0 < T; t0 += Lmax) {
     const int L = (T - t0) < Lmax ? (T - t0) : Lmax;
     if (threadIdx.x < kMaxStepBlock) sm.part[threadIdx.x] = 0.0f;
-    __syncthreads();
-
+    // the block's first tile: staged now (resident tiles stay staged)
+    if (!resident && (int)blockIdx.x < num_tiles) {
+      __syncthreads();
+      stage_load(nx, p, blockIdx.x * kTileVoxels);
+      stage_store(sm, nx);
+    } else {
+      __syncthreads();
+    }
     for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
       const int v0 = tile * kTileVoxels;
       const int nv = min(kTileVoxels, V - v0);
-      if (!resident) stage_tile(sm, p, v0);
-      for (int r0 = 0; r0 < L; r0 += kRound, ++round) {
-        const int R = (L - r0) < kRound ? (L - r0) : kRound;
-        const int buf = round & 1;
-        if (producer) {
-          if (round >= 2) named_sync(kBarEmpty + buf, kThreads);
-          produce(sm, p, v0, nv, t0 + r0, R, buf);
-          named_arrive(kBarFull + buf, kThreads);
-        } else {
-          named_sync(kBarFull + buf, kThreads);
-          consume(sm, p, v0, nv, t0 + r0, R, buf, r0);
-          named_arrive(kBarEmpty + buf, kThreads);
-        }
-      }
+      const int nt = tile + (int)gridDim.x;
+      const bool more = !resident && nt < num_tiles;
+      load_history(h, sm, p, t0, L < kRound ? L : kRound);
+      visit_tile(sm, p, v0, nv, t0, L, h, more ? &p : nullptr, nt * kTileVoxels, nx);
       if (!resident) {
-        __syncthreads();
         unstage_tile(sm, p, v0);
+        if (more) {
+          __syncthreads();  // every thread's chain state is out before the next tile's lands
+          stage_store(sm, nx);
+        }
       }
     }
     __syncthreads();
@@ -319,53 +365,55 @@ __global__ void __launch_bounds__(kThreads, 2) forward_stream_kernel(FwdArgs p) 
 // L = the smallest min(dmin, kMaxStepBlock) of any scenario. Each tile writes
 // its own per-step max-regularisation partial, stepsum_part[t * part_stride +
 // tile of the scenario], so the step metrics of every scenario sum the same
-// partials in the same order.
+// partials in the same order. A visit's last round issues the staging loads
+// of the CTA's next live tile (whatever its scenario).
 __global__ void __launch_bounds__(kThreads, 2) forward_batch_kernel(FwdBatch B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   __shared__ FwdArgs sp;
-  const bool producer = threadIdx.x < kProducers;
   int Lmax = kMaxStepBlock;
   for (int s = 0; s < B.nscn; ++s) {
     int dmin = B.scns[s].dmin[0];
     if (dmin < 1) dmin = 1;
     if (dmin < Lmax) Lmax = dmin;
   }
-  int cur = -1;
-  int round = 0;
+  float h[kLsItems][kRound + 1][3];
+  StageRegs nx;
+  // the CTA's first tile at or after list index `from` whose scenario still runs at step t0
+  auto next_live = [&](int from, int t0) {
+    int tile = from;
+    while (tile < B.ntiles && t0 >= B.scns[B.tiles[tile].x].T) tile += gridDim.x;
+    return tile;
+  };
   unsigned int barrier_number = 0;
   for (int t0 = 0; t0 < B.Tmax; t0 += Lmax) {
-    for (int tile = blockIdx.x; tile < B.ntiles; tile += gridDim.x) {
+    int tile = next_live(blockIdx.x, t0);
+    __syncthreads();
+    if (tile < B.ntiles) {
       const int2 tl = B.tiles[tile];
+      stage_load(nx, B.scns[tl.x], tl.y);
+      stage_store(sm, nx);
+    }
+    while (tile < B.ntiles) {
+      const int2 tl = B.tiles[tile];
+      if (threadIdx.x == 0) sp = B.scns[tl.x];
+      if (threadIdx.x < kMaxStepBlock) sm.part[threadIdx.x] = 0.0f;
       __syncthreads();
-      if (tl.x != cur) {
-        if (threadIdx.x == 0) sp = B.scns[tl.x];
-        cur = tl.x;
-        __syncthreads();
-      }
-      if (t0 >= sp.T) continue;  // uniform per CTA
       const int L = (sp.T - t0) < Lmax ? (sp.T - t0) : Lmax;
       const int v0 = tl.y;
       const int nv = min(kTileVoxels, sp.V - v0);
-      if (threadIdx.x < kMaxStepBlock) sm.part[threadIdx.x] = 0.0f;
-      stage_tile(sm, sp, v0);
-      for (int r0 = 0; r0 < L; r0 += kRound, ++round) {
-        const int R = (L - r0) < kRound ? (L - r0) : kRound;
-        const int buf = round & 1;
-        if (producer) {
-          if (round >= 2) named_sync(kBarEmpty + buf, kThreads);
-          produce(sm, sp, v0, nv, t0 + r0, R, buf);
-          named_arrive(kBarFull + buf, kThreads);
-        } else {
-          named_sync(kBarFull + buf, kThreads);
-          consume(sm, sp, v0, nv, t0 + r0, R, buf, r0);
-          named_arrive(kBarEmpty + buf, kThreads);
-        }
-      }
-      __syncthreads();
+      const int nt = next_live(tile + (int)gridDim.x, t0);
+      const bool more = nt < B.ntiles;
+      const int2 ntl = more ? B.tiles[nt] : make_int2(0, 0);
+      load_history(h, sm, sp, t0, L < kRound ? L : kRound);
+      visit_tile(sm, sp, v0, nv, t0, L, h, more ? &B.scns[ntl.x] : nullptr, ntl.y, nx);
       unstage_tile(sm, sp, v0);
+      __syncthreads();  // the last round's regularisation terms are in part[]
       if ((int)threadIdx.x < L)
         sp.stepsum_part[(size_t)(t0 + threadIdx.x) * sp.part_stride + v0 / kTileVoxels] = sm.part[threadIdx.x];
+      __syncthreads();  // chain state and partials are out, sp is free, before the next tile lands
+      if (more) stage_store(sm, nx);
+      tile = nt;
     }
     if (t0 + Lmax < B.Tmax) {
       if (!grid_barrier(B.barrier, barrier_number++, B.status)) return;
