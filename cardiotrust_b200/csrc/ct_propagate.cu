@@ -496,6 +496,10 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
   const int Lmax = dmin < kMaxStepBlock ? dmin : kMaxStepBlock;
   // rows a round reads: [tr0 - dmax - 1, tr0 + kRound - 1 - dmin]; plus kRound rows staged ahead
   const bool use_ring = (dmax - dmin + kRound + 1) + kRound <= kRingRows;
+  // rows a block reads: [t0 - dmax - 1, t0 + L - 1 - dmin], all produced before the block; when they
+  // fit the ring together, they are staged once at the block's start (one wait per block instead of
+  // one per round)
+  const bool stage_block = use_ring && (dmax - dmin + Lmax + 1) <= kRingRows;
 
   // ---- set-up: gains (transposed, masked), control, halo list, zeroed ring
   for (int e = threadIdx.x; e < kGainCols * kTileVoxels; e += blockDim.x) {
@@ -551,7 +555,17 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
       const int buf = round & 1;
       const int top = tr0 + R - 1 - dmin;  // newest history row this round reads
       if (producer) {
-        if (use_ring) {
+        if (stage_block) {
+          if (r0 == 0) {
+            const int top_blk = t0 + L - 1 - dmin;  // newest history row the block reads
+            if (top_blk > staged_top) {
+              stage_rows(sm, p, nh, staged_top + 1, top_blk);
+              staged_top = top_blk;
+            }
+            cp_async_commit_wait_all();
+            named_sync(kBarProducers, kProducers);  // the block's ring rows visible to all producers
+          }
+        } else if (use_ring) {
           if (r0 == 0 && top > staged_top) {  // first round of a block: rows produced in the previous block
             stage_rows(sm, p, nh, staged_top + 1, top);
             staged_top = top;
