@@ -59,6 +59,7 @@ constexpr int kThreads = kProducers + kConsumers;
 constexpr int kBarFull = 1;   // named barriers kBarFull + buffer, kBarEmpty + buffer (resident form)
 constexpr int kBarEmpty = 3;
 constexpr int kItemsPerProducer = (kTileItems + kProducers - 1) / kProducers;  // resident form
+static_assert(kRound == 2, "the producers' fast paths step two chains");
 
 // Streaming forms (a CTA walks several tiles, re-staging each per block of steps). All 192 threads
 // take both roles in turn: producers, one thread per (voxel, offset) item (4-5 items each), then
@@ -173,7 +174,22 @@ __device__ __forceinline__ void unstage_tile(Smem& sm, const FwdArgs& p, int v0)
 // j_i + b] (rows before t = 0 read as zero, prediction.rs:68-77). Every row read within a block of
 // L <= dmin steps is older than the block, so these loads may be issued at any time in the block.
 __device__ __forceinline__ void load_history(float (&h)[kLsItems][kRound + 1][3], const Smem& sm, const FwdArgs& p,
-                                             int tr0, int R) {
+                                             int tr0, int R, int dmax) {
+  if (R == kRound && tr0 - dmax - 1 >= 0) {
+    // every row exists: unpredicated loads (an absent neighbour reads column 0; its values are unused)
+#pragma unroll
+    for (int i = 0; i < kLsItems; ++i) {
+      const int e = threadIdx.x + i * kThreads;
+      const int jb = e < kTileItems ? sm.j[e] : -1;
+      const int d = jb >= 0 ? sm.d[e] : dmax;  // absent: an old row, values unused
+      const float* row = p.X + (size_t)(tr0 - d - 1) * p.S + (jb >= 0 ? jb : 0);
+#pragma unroll
+      for (int q = 0; q <= kRound; ++q)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) h[i][q][b] = row[(size_t)q * p.S + b];
+    }
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < kLsItems; ++i) {
     const int e = threadIdx.x + i * kThreads;
@@ -202,6 +218,36 @@ __device__ __forceinline__ void produce(Smem& sm, const FwdArgs& p, int v0, int 
       ck_s = tc - tr0;
       ck_row = p.ckpt + (size_t)((tc + 1) / p.ckpt_k) * p.V * kGainCols + (size_t)v0 * kGainCols;
     }
+  }
+  if (R == kRound && ck_s < 0 && !(tr0 <= p.T - 2 && p.T - 2 < tr0 + kRound)) {
+    // common round: no per-element checks (same arithmetic)
+#pragma unroll
+    for (int i = 0; i < kLsItems; ++i) {
+      const int e = threadIdx.x + i * kThreads;
+      if (e >= kTileItems) break;
+      const int vl = e / kOffsets;
+      const int n = e - vl * kOffsets;
+      float* st = sm.ap_state + vl * kGainCols + 3 * n;
+      float* out0 = sm.ap_out[0] + vl * kApPitch + 3 * n;
+      if (sm.j[e] >= 0) {
+        const float c = sm.c[e];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          float a = fmaf(c, h[i][1][b] - st[b], h[i][0][b]);
+          out0[b] = a;
+          a = fmaf(c, h[i][2][b] - a, h[i][1][b]);
+          out0[kTileVoxels * kApPitch + b] = a;
+          st[b] = a;
+        }
+      } else {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          out0[b] = 0.0f;
+          out0[kTileVoxels * kApPitch + b] = 0.0f;
+        }
+      }
+    }
+    return;
   }
 #pragma unroll
   for (int i = 0; i < kLsItems; ++i) {
@@ -282,7 +328,7 @@ __device__ __forceinline__ void regularise(Smem& sm, const FwdArgs& p, int nv, i
 // One visit of a tile: L steps from t0 in rounds of kRound. `h` holds the first round's history on
 // entry; with `next` set, the last round's consumer phase also issues the next tile's staging loads
 // into `nx` (stored by the caller after this visit).
-__device__ __forceinline__ void visit_tile(Smem& sm, const FwdArgs& p, int v0, int nv, int t0, int L,
+__device__ __forceinline__ void visit_tile(Smem& sm, const FwdArgs& p, int v0, int nv, int t0, int L, int dmax,
                                            float (&h)[kLsItems][kRound + 1][3], const FwdArgs* next, int next_v0,
                                            StageRegs& nx) {
   for (int r0 = 0; r0 < L; r0 += kRound) {
@@ -291,7 +337,7 @@ __device__ __forceinline__ void visit_tile(Smem& sm, const FwdArgs& p, int v0, i
     __syncthreads();
     if (r0 + kRound < L) {
       const int Rn = (L - r0 - kRound) < kRound ? (L - r0 - kRound) : kRound;
-      load_history(h, sm, p, t0 + r0 + kRound, Rn);
+      load_history(h, sm, p, t0 + r0 + kRound, Rn, dmax);
     } else if (next) {
       stage_load(nx, *next, next_v0);
     }
@@ -310,6 +356,7 @@ __global__ void __launch_bounds__(kThreads, 2) forward_stream_kernel(FwdArgs p) 
   const bool resident = num_tiles <= (int)gridDim.x;  // this CTA owns at most one tile
   int dmin = p.dmin[0];
   if (dmin < 1) dmin = 1;
+  const int dmax = p.dmin[1] > dmin ? p.dmin[1] : dmin;
   const int Lmax = dmin < kMaxStepBlock ? dmin : kMaxStepBlock;
   float h[kLsItems][kRound + 1][3];
   StageRegs nx;
@@ -335,8 +382,8 @@ __global__ void __launch_bounds__(kThreads, 2) forward_stream_kernel(FwdArgs p) 
       const int nv = min(kTileVoxels, V - v0);
       const int nt = tile + (int)gridDim.x;
       const bool more = !resident && nt < num_tiles;
-      load_history(h, sm, p, t0, L < kRound ? L : kRound);
-      visit_tile(sm, p, v0, nv, t0, L, h, more ? &p : nullptr, nt * kTileVoxels, nx);
+      load_history(h, sm, p, t0, L < kRound ? L : kRound, dmax);
+      visit_tile(sm, p, v0, nv, t0, L, dmax, h, more ? &p : nullptr, nt * kTileVoxels, nx);
       if (!resident) {
         unstage_tile(sm, p, v0);
         if (more) {
@@ -405,8 +452,9 @@ __global__ void __launch_bounds__(kThreads, 2) forward_batch_kernel(FwdBatch B) 
       const int nt = next_live(tile + (int)gridDim.x, t0);
       const bool more = nt < B.ntiles;
       const int2 ntl = more ? B.tiles[nt] : make_int2(0, 0);
-      load_history(h, sm, sp, t0, L < kRound ? L : kRound);
-      visit_tile(sm, sp, v0, nv, t0, L, h, more ? &B.scns[ntl.x] : nullptr, ntl.y, nx);
+      const int dmax = max(sp.dmin[1], 1);
+      load_history(h, sm, sp, t0, L < kRound ? L : kRound, dmax);
+      visit_tile(sm, sp, v0, nv, t0, L, dmax, h, more ? &B.scns[ntl.x] : nullptr, ntl.y, nx);
       unstage_tile(sm, sp, v0);
       __syncthreads();  // the last round's regularisation terms are in part[]
       if ((int)threadIdx.x < L)
@@ -595,6 +643,41 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
             ck_row = p.ckpt + (size_t)((tc + 1) / p.ckpt_k) * p.V * kGainCols + (size_t)v0 * kGainCols;
           }
         }
+        // common round: full length, every history row from the ring at t >= 0, no checkpoint and
+        // no ap_last step: the chains without per-element checks (same arithmetic)
+        const bool fast = use_ring && R == kRound && tr0 - dmax - 1 >= 0 && ck_s < 0 &&
+                          !(tr0 <= T - 2 && T - 2 < tr0 + kRound);
+        if (fast) {
+#pragma unroll
+          for (int i = 0; i < kItemsPerProducer; ++i) {
+            const int e = threadIdx.x + i * kProducers;
+            if (e >= kTileItems) break;
+            const int vl = e / kOffsets;
+            const int n = e - vl * kOffsets;
+            float* out0 = sm.ap_out[buf][0] + vl * kGainCols + 3 * n;
+            if (hs[i] >= 0) {
+              const int base = tr0 - dd[i] - 1;
+              const float* h0 = &sm.ring[base & (kRingRows - 1)][3 * hs[i]];
+              const float* h1 = &sm.ring[(base + 1) & (kRingRows - 1)][3 * hs[i]];
+              const float* h2 = &sm.ring[(base + 2) & (kRingRows - 1)][3 * hs[i]];
+#pragma unroll
+              for (int b = 0; b < 3; ++b) {
+                const float x0 = h0[b], x1 = h1[b], x2 = h2[b];
+                float a = fmaf(cc[i], x1 - st[i][b], x0);
+                out0[b] = a;
+                a = fmaf(cc[i], x2 - a, x1);
+                out0[kTileVoxels * kGainCols + b] = a;
+                st[i][b] = a;
+              }
+            } else {
+#pragma unroll
+              for (int b = 0; b < 3; ++b) {
+                out0[b] = 0.0f;
+                out0[kTileVoxels * kGainCols + b] = 0.0f;
+              }
+            }
+          }
+        } else {
 #pragma unroll
         for (int i = 0; i < kItemsPerProducer; ++i) {
           const int e = threadIdx.x + i * kProducers;
@@ -639,6 +722,7 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
 #pragma unroll
                 for (int b = 0; b < 3; ++b) out0[s2 * (kTileVoxels * kGainCols) + b] = 0.0f;
           }
+        }
         }
         named_arrive(kBarFull + buf, kThreads);
       } else {
