@@ -73,6 +73,9 @@ struct ct_scn {
   ct::PostBuffers post{};
   ct::PostPlan post_plan{};
   bool post_arrays = false;  // CT_FIELD_STATES_* / CT_FIELD_ACTIVATION_TIMES hold results
+  // field transfers: device perm and a staging buffer of S * 78 words (voxel reordering on the device)
+  int32_t* perm_dev = nullptr;
+  uint32_t* xfer = nullptr;
   // ct_calculate_final: grid types and numbers [2, cells], threshold histogram, results (grown on demand)
   int64_t final_cells = 0;
   int32_t* final_grid = nullptr;
@@ -656,14 +659,42 @@ int copy_down_expanded(ct_scn* s, float* dst, const float* src) {
   return CT_OK;
 }
 
-// Per-voxel row blocks (rows_per_voxel x row_len elements) in device order -> reference order.
 template <typename T>
-int copy_down_rows(ct_scn* s, T* dst, const T* src, int64_t rows_per_voxel, int64_t row_len) {
+int copy_down_rows_host(ct_scn* s, T* dst, const T* src, int64_t rows_per_voxel, int64_t row_len) {
   std::vector<T> tmp((size_t)(s->d.V * rows_per_voxel * row_len));
   int rc = copy_down(s, tmp.data(), src, sizeof(T) * tmp.size());
   if (rc) return rc;
   scatter_rows(dst, tmp.data(), s->perm, rows_per_voxel, row_len);
   return CT_OK;
+}
+
+// Staging buffer and device perm for reordering transfers on the device (allocated on first use).
+int ensure_xfer(ct_scn* s) {
+  if (s->xfer) return CT_OK;
+  int rc = alloc(s, &s->perm_dev, s->d.V);
+  if (!rc) rc = upload(s, s->perm_dev, s->perm.data(), sizeof(int32_t) * s->perm.size());
+  if (!rc) rc = alloc(s, &s->xfer, s->d.S * kGainCols);
+  if (rc) {
+    release(s, s->perm_dev);
+    release(s, s->xfer);
+    s->perm_dev = nullptr;
+    s->xfer = nullptr;
+  }
+  return rc;
+}
+
+// Per-voxel row blocks (rows_per_voxel x row_len elements) in device order -> reference order:
+// scattered on the device into the staging buffer, then one copy to the host.
+template <typename T>
+int copy_down_rows(ct_scn* s, T* dst, const T* src, int64_t rows_per_voxel, int64_t row_len) {
+  static_assert(sizeof(T) == 4, "32-bit elements");
+  if (rows_per_voxel * row_len <= kGainCols * 3 && ensure_xfer(s) == CT_OK) {
+    const int64_t words = rows_per_voxel * row_len;
+    CT_CUDA(ct::launch_permute_blocks(src, s->xfer, s->perm_dev, s->d.V, words, false, s->ctx->stream),
+            "permute kernel");
+    return copy_down(s, dst, s->xfer, sizeof(T) * (size_t)(s->d.V * words));
+  }
+  return copy_down_rows_host(s, dst, src, rows_per_voxel, row_len);
 }
 
 // `rows` rows of S states in device order -> reference order.
@@ -1224,11 +1255,16 @@ int ct_write_field(ct_scn* scn, int field, const void* src, size_t nbytes) {
     case CT_FIELD_MEASUREMENTS_ACTUAL: dst = d.meas; break;
     default: return fail(CT_ERR_INVALID_ARGUMENT, "field %d is read-only", field);
   }
-  // reorder into device voxel order (measurements are in sensor space and need no reordering)
-  std::vector<unsigned char> staged;
-  const void* from = src;
-  if (field != CT_FIELD_MEASUREMENTS_ACTUAL) {
-    staged.resize(nbytes);
+  // reorder into device voxel order on the device (measurements are in sensor space: no reordering)
+  if (field == CT_FIELD_MEASUREMENTS_ACTUAL) {
+    CT_CUDA(cudaMemcpyAsync(dst, src, nbytes, cudaMemcpyHostToDevice, scn->ctx->stream), "write field");
+  } else if (ensure_xfer(scn) == CT_OK) {
+    const int64_t words = field == CT_FIELD_GAINS ? 3 * kGainCols : kOffsets;
+    CT_CUDA(cudaMemcpyAsync(scn->xfer, src, nbytes, cudaMemcpyHostToDevice, scn->ctx->stream), "write field");
+    CT_CUDA(ct::launch_permute_blocks(scn->xfer, dst, scn->perm_dev, d.V, words, true, scn->ctx->stream),
+            "permute kernel");
+  } else {
+    std::vector<unsigned char> staged(nbytes);
     if (field == CT_FIELD_GAINS)
       gather_rows(reinterpret_cast<float*>(staged.data()), static_cast<const float*>(src), scn->perm, 3, kGainCols);
     else if (field == CT_FIELD_COEFS)
@@ -1236,9 +1272,9 @@ int ct_write_field(ct_scn* scn, int field, const void* src, size_t nbytes) {
     else
       gather_rows(reinterpret_cast<int32_t*>(staged.data()), static_cast<const int32_t*>(src), scn->perm, 1,
                   kOffsets);
-    from = staged.data();
+    CT_CUDA(cudaMemcpyAsync(dst, staged.data(), nbytes, cudaMemcpyHostToDevice, scn->ctx->stream), "write field");
+    CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "write field");
   }
-  CT_CUDA(cudaMemcpyAsync(dst, from, nbytes, cudaMemcpyHostToDevice, scn->ctx->stream), "write field");
   if (field == CT_FIELD_DELAYS) CT_CUDA(ct::launch_min_delay(d, scn->ctx->stream), "min delay kernel");
   CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "write field");
   return CT_OK;

@@ -236,6 +236,10 @@ struct UpdateScalars {
 cudaError_t launch_update(DeviceScenario& d, const UpdateScalars& s, cudaStream_t stream);
 cudaError_t launch_min_delay(DeviceScenario& d, cudaStream_t stream);
 
+// Voxel blocks of `words` 32-bit words between reference and device voxel order (perm[u] = the
+// reference voxel of device voxel u): gather dst[u] = src[perm[u]], else scatter dst[perm[u]] = src[u].
+cudaError_t launch_permute_blocks(const void* src, void* dst, const int32_t* perm, int64_t V, int64_t words,
+                                  bool gather, cudaStream_t stream);
 // Expand the deduplicated [V,78] all-pass/fir/iir state into the reference [S,78] layout.
 cudaError_t launch_expand_rows(const float* src, float* dst, int64_t V, cudaStream_t stream);
 // Last-step maximum regularisation [S] from X[T-1].

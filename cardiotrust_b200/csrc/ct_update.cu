@@ -331,6 +331,34 @@ cudaError_t launch_step_metrics_parts(DeviceScenario& d, const float* part, int 
   return cudaGetLastError();
 }
 
+// Voxel blocks of `words` 32-bit words: gather dst[u] = src[perm[u]] (reference -> device order) or
+// scatter dst[perm[u]] = src[u] (device -> reference order).
+template <bool kGather>
+__global__ void permute_blocks_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                                      const int32_t* __restrict__ perm, int64_t V, int64_t words) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V * words) return;
+  const int64_t u = i / words, w = i - u * words;
+  const int64_t r = perm[u];
+  if (kGather)
+    dst[i] = src[r * words + w];
+  else
+    dst[r * words + w] = src[i];
+}
+
+cudaError_t launch_permute_blocks(const void* src, void* dst, const int32_t* perm, int64_t V, int64_t words,
+                                  bool gather, cudaStream_t stream) {
+  const int64_t n = V * words;
+  const unsigned grid = (unsigned)((n + 255) / 256);
+  if (gather)
+    permute_blocks_kernel<true><<<grid, 256, 0, stream>>>(static_cast<const uint32_t*>(src), static_cast<uint32_t*>(dst),
+                                                          perm, V, words);
+  else
+    permute_blocks_kernel<false><<<grid, 256, 0, stream>>>(static_cast<const uint32_t*>(src),
+                                                           static_cast<uint32_t*>(dst), perm, V, words);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_expand_rows(const float* src, float* dst, int64_t V, cudaStream_t stream) {
   expand_rows_kernel<<<blocks(3 * V * kGainCols, 256), 256, 0, stream>>>(src, dst, V);
   return cudaGetLastError();
