@@ -308,6 +308,7 @@ def post_run_section(alg, eng, scn, stream, hbm_peak, prec):
         fm = eng.calculate_final(scn.types_truth, scn.numbers)
         fms.append((time.perf_counter() - t0) * 1000.0)
     final_ms = min(fms)
+    model = model_construction(alg, eng, scn)
     loop_epochs = 5
     a = dataclasses.replace(algorithm_config(alg), epochs=loop_epochs, learning_rate_reduction_interval=2,
                             learning_rate_reduction_factor=0.5)
@@ -324,10 +325,48 @@ def post_run_section(alg, eng, scn, stream, hbm_peak, prec):
                           "dice": fm.dice, "iou": fm.iou,
                           "note": "wall clock of the C call (best of 5 after the first): grid upload, states scan, "
                                   "threshold sweep, read-back"},
+        "model_construction": model,
         "scenario_loop": {"epochs": loop_epochs, "epochs_run": summ["epochs_run"],
                           "scenario_epochs_per_s": loop_epochs / loop_s,
                           "note": "ct_run_model_based wall clock: schedule, one summary read-back per epoch"},
     }
+
+
+def model_construction(alg, eng, scn):
+    """The step before the epoch on the headline workload: the Biot-Savart measurement matrix and the
+    delay arrays built on the device (wall clock of the synchronous C calls, best of 5 after the
+    first) against the host builder's vectorised numpy restatement of the same loops."""
+    import numpy as np
+
+    from cardiotrust_b200 import scenario as sc
+
+    spec = scn.spec
+    sd = alg.SpatialDescription.from_scenario(scn)
+
+    def best(fn, n=5):
+        fn()
+        ts = []
+        for _ in range(n):
+            t0 = time.perf_counter()
+            fn()
+            ts.append((time.perf_counter() - t0) * 1000.0)
+        return min(ts)
+
+    fill_ms = best(lambda: eng.set_measurement_matrix(sd))
+    h_ms = best(lambda: alg.measurement_matrix(eng.ctx, sd))
+    d_ms = best(lambda: alg.delay_samples(eng.ctx, sd))
+    host_h_ms = best(lambda: sc._measurement_matrix(spec, scn.types_model, scn.numbers, scn.positions_mm,
+                                                    scn.sensor_positions_mm, scn.sensor_orientations), n=2)
+    host_d_ms = best(lambda: sc._delay_samples(scn.types_model, scn.numbers, scn.positions_mm, spec.velocity_m_per_s,
+                                               spec.sample_rate_hz), n=2)
+    H = alg.measurement_matrix(eng.ctx, sd)
+    samples, delays, coefs = alg.delay_samples(eng.ctx, sd)
+    same = bool(np.array_equal(H, scn.measurement_matrix) and np.array_equal(samples, scn.model.initial_delays)
+                and np.array_equal(delays, scn.model.delays) and np.array_equal(coefs, scn.model.coefs))
+    return {"lead_field_into_scenario_ms": fill_ms, "lead_field_to_host_ms": h_ms, "delay_arrays_to_host_ms": d_ms,
+            "host_builder_lead_field_ms": host_h_ms, "host_builder_delays_ms": host_d_ms,
+            "bit_identical_to_host_builder": same, "matrix_bytes": int(H.nbytes),
+            "note": "wall clock of the synchronous C calls (uploads, kernel, operand splits or read-back)"}
 
 
 def _noisy_scenario(alg, sc, ctx, spec):

@@ -118,6 +118,9 @@ EXPORTED = [
     "ct_batch_run_model_based",
     "ct_calculate_plotting_arrays",
     "ct_calculate_final",
+    "ct_measurement_matrix",
+    "ct_delay_samples",
+    "ct_scenario_set_measurement_matrix",
 ]
 
 PHASES = ["forward", "measure", "map_residuals", "derive", "step_metrics", "update"]
@@ -197,6 +200,25 @@ class CtFinalMetrics(ctypes.Structure):
     ]
 
 
+class CtSpatialDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int64),
+        ("ny", ctypes.c_int64),
+        ("nz", ctypes.c_int64),
+        ("voxel_types", _ip),
+        ("voxel_numbers", _ip),
+        ("voxel_positions_mm", _fp),
+        ("voxel_size_mm", ctypes.c_float),
+        ("sample_rate_hz", ctypes.c_float),
+        ("propagation_velocities_m_per_s", _fp),
+        ("num_sensors", ctypes.c_int64),
+        ("num_beats", ctypes.c_int64),
+        ("sensor_positions_mm", _fp),
+        ("sensor_orientations", _fp),
+        ("sensor_array_offsets_mm", _fp),
+    ]
+
+
 class CtError(RuntimeError):
     """A non-zero ct_status, with the library's message."""
 
@@ -255,6 +277,9 @@ def load(path: pathlib.Path = LIB_PATH) -> ctypes.CDLL:
     lib.ct_calculate_plotting_arrays.argtypes = [vp, ctypes.c_float]
     lib.ct_calculate_final.argtypes = [vp, _ip, _ip, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                        ctypes.POINTER(CtFinalMetrics)]
+    lib.ct_measurement_matrix.argtypes = [vp, ctypes.POINTER(CtSpatialDesc), _fp, ctypes.c_size_t]
+    lib.ct_delay_samples.argtypes = [vp, ctypes.POINTER(CtSpatialDesc), _fp, _ip, _fp, ctypes.c_int64]
+    lib.ct_scenario_set_measurement_matrix.argtypes = [vp, ctypes.POINTER(CtSpatialDesc)]
     for name in EXPORTED:
         getattr(lib, name)  # AttributeError if a declared symbol is not exported
     return lib

@@ -152,13 +152,21 @@ class EpochEngine:
         measurements=None,
         num_batch_slots: int = 1,
         algorithm: Optional[Algorithm] = None,
+        spatial: Optional["SpatialDescription"] = None,
     ):
         self.ctx = ctx
         self.algorithm = algorithm or Algorithm()
-        H = _f32(measurement_matrix)
-        if H.ndim != 3:
-            raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, "measurement_matrix must be [beats, sensors, states]")
-        B, M, S = H.shape
+        if measurement_matrix is None:
+            # the lead field is computed on the device from the spatial description
+            if spatial is None:
+                raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, "measurement_matrix or spatial is required")
+            H = None
+            B, M, S = spatial.num_beats, spatial.num_sensors, _f32(gains).shape[0]
+        else:
+            H = _f32(measurement_matrix)
+            if H.ndim != 3:
+                raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, "measurement_matrix must be [beats, sensors, states]")
+            B, M, S = H.shape
         u = _f32(control_function)
         keep = dict(
             gains=_f32(gains),
@@ -186,7 +194,7 @@ class EpochEngine:
         d.coefs = fptr(keep["coefs"])
         d.delays = iptr(keep["delays"])
         d.initial_delays = fptr(keep["init"])
-        d.measurement_matrix = fptr(H)
+        d.measurement_matrix = fptr(H) if H is not None else None
         d.control_matrix = fptr(keep["ctrl"])
         d.control_function = fptr(u)
         d.measurements = fptr(keep["meas"]) if keep["meas"] is not None else None
@@ -194,6 +202,14 @@ class EpochEngine:
         ca = self.algorithm.to_ct()
         check(lib().ct_scenario_create(ctx.handle, ctypes.byref(d), ctypes.byref(ca), ctypes.byref(self._h)))
         self.dims = dict(S=S, V=V, M=M, T=u.shape[0], B=B, NB=int(num_batch_slots))
+        if H is None:
+            self.set_measurement_matrix(spatial)
+
+    def set_measurement_matrix(self, spatial: "SpatialDescription") -> None:
+        """The Biot-Savart measurement matrix computed on the device straight into this scenario
+        (``ct_scenario_set_measurement_matrix``): no [B, M, S] host array crosses PCIe."""
+        desc, _keep = spatial.to_ct()
+        check(lib().ct_scenario_set_measurement_matrix(self._h, ctypes.byref(desc)))
 
     # -- parameters
     def set_algorithm(self, algorithm: Algorithm) -> None:
@@ -343,7 +359,9 @@ class EpochEngine:
 
     @classmethod
     def from_scenario(cls, ctx: Context, scn, *, truth: bool = False, num_batch_slots: int = 1,
-                      algorithm: Optional[Algorithm] = None) -> "EpochEngine":
+                      algorithm: Optional[Algorithm] = None, device_lead_field: bool = False) -> "EpochEngine":
+        """An engine for a built scenario; ``device_lead_field`` computes the measurement matrix on the
+        device from the scenario's geometry instead of copying ``scn.measurement_matrix``."""
         p = scn.truth if truth else scn.model
         return cls(
             ctx,
@@ -352,13 +370,120 @@ class EpochEngine:
             coefs=p.coefs,
             delays=p.delays,
             initial_delays=p.initial_delays,
-            measurement_matrix=scn.measurement_matrix,
+            measurement_matrix=None if device_lead_field else scn.measurement_matrix,
+            spatial=SpatialDescription.from_scenario(scn, truth=truth) if device_lead_field else None,
             control_matrix=scn.control_matrix,
             control_function=scn.control_function,
             measurements=scn.measurements,
             num_batch_slots=num_batch_slots,
             algorithm=algorithm,
         )
+
+
+# ------------------------------------------------------------------------------------------
+# Model construction on the device
+
+
+@dataclasses.dataclass
+class SpatialDescription:
+    """The parts of the reference's ``SpatialDescription`` (src/core/model/spatial.rs) and model
+    config that the measurement matrix and the delay arrays are built from."""
+
+    voxel_types: np.ndarray  # [nx,ny,nz] VoxelType discriminants
+    voxel_numbers: np.ndarray  # [nx,ny,nz] state index 3v, -1 = None
+    voxel_positions_mm: np.ndarray  # [nx,ny,nz,3]
+    voxel_size_mm: float
+    sensor_positions_mm: np.ndarray  # [M,3]
+    sensor_orientations: np.ndarray  # [M,3]
+    sensor_array_offsets_mm: np.ndarray  # [B,3]
+    sample_rate_hz: float = 2000.0
+    propagation_velocities_m_per_s: Optional[np.ndarray] = None  # [10] per VoxelType
+
+    @property
+    def num_sensors(self) -> int:
+        return int(np.asarray(self.sensor_positions_mm).shape[0])
+
+    @property
+    def num_beats(self) -> int:
+        return int(np.asarray(self.sensor_array_offsets_mm).reshape(-1, 3).shape[0])
+
+    @property
+    def num_voxels(self) -> int:
+        t = np.asarray(self.voxel_types)
+        return int(((t >= 1) & (t <= 6)).sum())
+
+    def to_ct(self):
+        """(CtSpatialDesc, arrays it points into: keep them alive while the struct is used)."""
+        keep = dict(
+            t=np.ascontiguousarray(self.voxel_types, dtype=np.int32),
+            n=np.ascontiguousarray(self.voxel_numbers, dtype=np.int32),
+            p=np.ascontiguousarray(self.voxel_positions_mm, dtype=np.float32),
+            sp=np.ascontiguousarray(self.sensor_positions_mm, dtype=np.float32),
+            so=np.ascontiguousarray(self.sensor_orientations, dtype=np.float32),
+            off=np.ascontiguousarray(np.asarray(self.sensor_array_offsets_mm).reshape(-1, 3), dtype=np.float32),
+            vel=np.ascontiguousarray(np.zeros(10) if self.propagation_velocities_m_per_s is None
+                                     else self.propagation_velocities_m_per_s, dtype=np.float32),
+        )
+        if keep["t"].ndim != 3 or keep["n"].shape != keep["t"].shape or keep["p"].shape != keep["t"].shape + (3,):
+            raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, "voxel grid arrays must be [nx,ny,nz] and [nx,ny,nz,3]")
+        if keep["sp"].shape != keep["so"].shape or keep["sp"].ndim != 2 or keep["sp"].shape[1] != 3:
+            raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, "sensor arrays must be [M,3]")
+        if keep["vel"].shape != (10,):
+            raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, "propagation velocities must have 10 entries")
+        d = _lib.CtSpatialDesc()
+        d.nx, d.ny, d.nz = keep["t"].shape
+        d.voxel_types = iptr(keep["t"])
+        d.voxel_numbers = iptr(keep["n"])
+        d.voxel_positions_mm = fptr(keep["p"])
+        d.voxel_size_mm = float(self.voxel_size_mm)
+        d.sample_rate_hz = float(self.sample_rate_hz)
+        d.propagation_velocities_m_per_s = fptr(keep["vel"])
+        d.num_sensors = keep["sp"].shape[0]
+        d.num_beats = keep["off"].shape[0]
+        d.sensor_positions_mm = fptr(keep["sp"])
+        d.sensor_orientations = fptr(keep["so"])
+        d.sensor_array_offsets_mm = fptr(keep["off"])
+        return d, keep
+
+    @classmethod
+    def from_scenario(cls, scn, truth: bool = False) -> "SpatialDescription":
+        from . import scenario as sc
+
+        spec = scn.spec
+        return cls(
+            voxel_types=scn.types_truth if truth else scn.types_model,
+            voxel_numbers=scn.numbers,
+            voxel_positions_mm=scn.positions_mm,
+            voxel_size_mm=spec.voxel_size_mm,
+            sensor_positions_mm=scn.sensor_positions_mm,
+            sensor_orientations=scn.sensor_orientations,
+            sensor_array_offsets_mm=sc.array_offsets_mm(spec),
+            sample_rate_hz=spec.sample_rate_hz,
+            propagation_velocities_m_per_s=sc.velocities_by_type(spec),
+        )
+
+
+def measurement_matrix(ctx: Context, spatial: SpatialDescription) -> np.ndarray:
+    """``MeasurementMatrix::from_model_spatial_description`` (measurement.rs:66-123) on the device:
+    H [B, M, S] in reference state order."""
+    desc, _keep = spatial.to_ct()
+    out = np.empty((spatial.num_beats, spatial.num_sensors, 3 * spatial.num_voxels), np.float32)
+    check(lib().ct_measurement_matrix(ctx.handle, ctypes.byref(desc), fptr(out), out.nbytes))
+    return out
+
+
+def delay_samples(ctx: Context, spatial: SpatialDescription):
+    """``calculate_delay_samples_array`` (allpass/delay.rs:35-111) with the delays and coefficients of
+    ``APParameters::from_model_config`` (allpass.rs:86-100), on the device.
+    Returns (initial_delays f32, delays i32, coefs f32), each [V, 26]."""
+    desc, _keep = spatial.to_ct()
+    V = spatial.num_voxels
+    samples = np.empty((V, 26), np.float32)
+    delays = np.empty((V, 26), np.int32)
+    coefs = np.empty((V, 26), np.float32)
+    check(lib().ct_delay_samples(ctx.handle, ctypes.byref(desc), fptr(samples), iptr(delays), fptr(coefs),
+                                 samples.size))
+    return samples, delays, coefs
 
 
 # ------------------------------------------------------------------------------------------

@@ -19,7 +19,7 @@ LIB = PKG / "libcardiotrust_cuda.so"
 BUILD_DIR = PKG / "_build"
 
 SOURCES = ["ct_api.cu", "ct_propagate.cu", "ct_measure.cu", "ct_derive.cu", "ct_update.cu", "ct_umma.cu", "ct_adjoint.cu", "ct_plain.cu",
-           "ct_post.cu"]
+           "ct_post.cu", "ct_model.cu"]
 HEADERS = ["ct_internal.cuh", "ct_sync.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

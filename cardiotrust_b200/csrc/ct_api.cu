@@ -794,7 +794,7 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   if (T * S >= (int64_t(1) << 31) || S * kGainCols >= (int64_t(1) << 31) || B * M * S >= (int64_t(1) << 40))
     return fail(CT_ERR_NOT_SUPPORTED, "num_steps x num_states must stay below 2^31 (32-bit state indexing)");
   if (!desc->gains || !desc->output_state_indices || !desc->coefs || !desc->delays || !desc->initial_delays ||
-      !desc->measurement_matrix || !desc->control_matrix || !desc->control_function)
+      !desc->control_matrix || !desc->control_function)
     return fail(CT_ERR_INVALID_ARGUMENT, "a required array pointer is NULL");
   std::vector<int32_t> nbr;
   rc = validate_and_build_nbr(desc, nbr);
@@ -902,14 +902,14 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   // model arrays in device voxel order (uploads are synchronous on the context stream below,
   // so the host staging vectors outlive their copies)
   std::vector<float> h_gains((size_t)(S * kGainCols)), h_coefs((size_t)(V * kOffsets)),
-      h_init((size_t)(V * kOffsets)), h_ctrl((size_t)S), h_H((size_t)(B * M * S));
+      h_init((size_t)(V * kOffsets)), h_ctrl((size_t)S), h_H(desc->measurement_matrix ? (size_t)(B * M * S) : 0);
   std::vector<int32_t> h_nbr((size_t)(V * kOffsets)), h_delays((size_t)(V * kOffsets));
   gather_rows(h_gains.data(), desc->gains, s->perm, 3, kGainCols);
   gather_rows(h_coefs.data(), desc->coefs, s->perm, 1, kOffsets);
   gather_rows(h_init.data(), desc->initial_delays, s->perm, 1, kOffsets);
   gather_rows(h_delays.data(), desc->delays, s->perm, 1, kOffsets);
   gather_state_columns(h_ctrl.data(), desc->control_matrix, s->perm, 1);
-  gather_state_columns(h_H.data(), desc->measurement_matrix, s->perm, B * M);
+  if (desc->measurement_matrix) gather_state_columns(h_H.data(), desc->measurement_matrix, s->perm, B * M);
   for (int64_t u = 0; u < V; ++u)
     for (int n = 0; n < kOffsets; ++n) {
       const int32_t w = nbr[(size_t)s->perm[(size_t)u] * kOffsets + n];
@@ -921,7 +921,7 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   r = r ? r : upload(s, d.coefs, h_coefs.data(), sizeof(float) * V * kOffsets);
   r = r ? r : upload(s, d.delays, h_delays.data(), sizeof(int32_t) * V * kOffsets);
   r = r ? r : upload(s, d.init_delays, h_init.data(), sizeof(float) * V * kOffsets);
-  r = r ? r : upload(s, d.H, h_H.data(), sizeof(float) * B * M * S);
+  if (desc->measurement_matrix) r = r ? r : upload(s, d.H, h_H.data(), sizeof(float) * B * M * S);
   r = r ? r : upload(s, d.ctrl, h_ctrl.data(), sizeof(float) * S);
   if (d.fwd_ring) {
     r = r ? r : upload(s, d.halo, h_halo.data(), sizeof(int32_t) * h_halo.size());
@@ -939,6 +939,7 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
     cudaError_t e = cudaMemsetAsync(p, 0, bytes, st);
     if (e != cudaSuccess) r = cuda_fail(e, "memset");
   };
+  if (!desc->measurement_matrix) zero(d.H, sizeof(float) * B * M * S);  // ct_scenario_set_measurement_matrix fills it
   zero(d.X, sizeof(float) * T * S);
   zero(d.Y, sizeof(float) * B * T * M);
   zero(d.R, sizeof(float) * T * M);
@@ -2272,6 +2273,210 @@ int ct_calculate_final(ct_scn* scn, const int32_t* ground_truth_types, const int
   if (e != cudaSuccess) return cuda_fail(e, "final metrics");
   scn->launches += 4;
   return ct_sync(scn);
+}
+
+
+// ---- model construction on the device
+
+}  // extern "C"
+
+namespace {
+
+// Device buffers of one model-construction call, freed on every return path (cudaFree waits for
+// the device, so nothing in flight still uses them).
+struct TempBuffers {
+  std::vector<void*> ptrs;
+  ~TempBuffers() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <typename T>
+  cudaError_t get(T** p, int64_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, sizeof(T) * (size_t)(count > 0 ? count : 1));
+    if (e == cudaSuccess) {
+      ptrs.push_back(q);
+      *p = static_cast<T*>(q);
+    }
+    return e;
+  }
+};
+
+bool is_connectable(int32_t t) { return t >= 1 && t <= 6; }  // voxels.rs:690-700
+
+// The voxel grid of a spatial description: connectable cells must carry the voxel numbers
+// 0, 3, .., S-3 once each (the reference's numbering, voxels.rs:407-424). cell_of[v] = the cell
+// of voxel v.
+int check_grid(const ct_spatial_desc* g, std::vector<int64_t>& cell_of) {
+  if (!g->voxel_types || !g->voxel_numbers || !g->voxel_positions_mm)
+    return fail(CT_ERR_INVALID_ARGUMENT, "a voxel grid array is NULL");
+  if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0) return fail(CT_ERR_INVALID_ARGUMENT, "empty voxel grid");
+  if (g->nx * g->ny >= (int64_t(1) << 31) || g->nx * g->ny * g->nz >= (int64_t(1) << 31) / kOffsets)
+    return fail(CT_ERR_NOT_SUPPORTED, "voxel grid too large");
+  const int64_t cells = g->nx * g->ny * g->nz;
+  int64_t V = 0;
+  for (int64_t c = 0; c < cells; ++c) V += is_connectable(g->voxel_types[c]) ? 1 : 0;
+  if (V == 0) return fail(CT_ERR_INVALID_ARGUMENT, "the voxel grid has no connectable voxel");
+  cell_of.assign((size_t)V, -1);
+  for (int64_t c = 0; c < cells; ++c) {
+    if (!is_connectable(g->voxel_types[c])) continue;
+    const int32_t num = g->voxel_numbers[c];
+    if (num < 0 || num % 3 != 0 || num / 3 >= V || cell_of[(size_t)(num / 3)] >= 0)
+      return fail(CT_ERR_INVALID_ARGUMENT,
+                  "voxel number %d of connectable cell %lld: connectable cells must number 0, 3, .., %lld once each",
+                  num, (long long)c, (long long)(3 * V - 3));
+    cell_of[(size_t)(num / 3)] = c;
+  }
+  return CT_OK;
+}
+
+int check_sensors(const ct_spatial_desc* g) {
+  if (!g->sensor_positions_mm || !g->sensor_orientations || !g->sensor_array_offsets_mm)
+    return fail(CT_ERR_INVALID_ARGUMENT, "a sensor array is NULL");
+  if (g->num_sensors <= 0 || g->num_beats <= 0)
+    return fail(CT_ERR_INVALID_ARGUMENT, "num_sensors and num_beats must be positive");
+  return CT_OK;
+}
+
+// H [B, M, ldh] on the device from a voxel list (vpos[i], first column col[i]).
+int fill_lead_field(ct_ctx* ctx, const ct_spatial_desc* g, const std::vector<float>& vpos,
+                    const std::vector<int32_t>& col, float* H, int64_t ldh) {
+  const int64_t nv = (int64_t)col.size(), M = g->num_sensors, B = g->num_beats;
+  cudaStream_t st = ctx->stream;
+  TempBuffers tb;
+  float *dv = nullptr, *dsp = nullptr, *dso = nullptr, *doff = nullptr;
+  int32_t* dc = nullptr;
+  CT_CUDA(tb.get(&dv, 3 * nv), "cudaMalloc");
+  CT_CUDA(tb.get(&dc, nv), "cudaMalloc");
+  CT_CUDA(tb.get(&dsp, 3 * M), "cudaMalloc");
+  CT_CUDA(tb.get(&dso, 3 * M), "cudaMalloc");
+  CT_CUDA(tb.get(&doff, 3 * B), "cudaMalloc");
+  CT_CUDA(cudaMemcpyAsync(dv, vpos.data(), sizeof(float) * vpos.size(), cudaMemcpyHostToDevice, st), "upload");
+  CT_CUDA(cudaMemcpyAsync(dc, col.data(), sizeof(int32_t) * col.size(), cudaMemcpyHostToDevice, st), "upload");
+  CT_CUDA(cudaMemcpyAsync(dsp, g->sensor_positions_mm, sizeof(float) * 3 * M, cudaMemcpyHostToDevice, st), "upload");
+  CT_CUDA(cudaMemcpyAsync(dso, g->sensor_orientations, sizeof(float) * 3 * M, cudaMemcpyHostToDevice, st), "upload");
+  CT_CUDA(cudaMemcpyAsync(doff, g->sensor_array_offsets_mm, sizeof(float) * 3 * B, cudaMemcpyHostToDevice, st),
+          "upload");
+  CT_CUDA(ct::launch_lead_field(dv, dc, nv, dsp, dso, doff, M, B, ct::lead_field_factor(g->voxel_size_mm), H, ldh,
+                                ctx->num_sms, st),
+          "lead field kernel");
+  CT_CUDA(cudaStreamSynchronize(st), "lead field");
+  return CT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ct_measurement_matrix(ct_ctx* ctx, const ct_spatial_desc* desc, float* out, size_t nbytes) {
+  if (!ctx || !desc || !out) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::vector<int64_t> cell_of;
+  int rc = check_grid(desc, cell_of);
+  if (!rc) rc = check_sensors(desc);
+  if (rc) return rc;
+  const int64_t V = (int64_t)cell_of.size(), S = 3 * V, M = desc->num_sensors, B = desc->num_beats;
+  if (B * M * S >= (int64_t(1) << 40)) return fail(CT_ERR_NOT_SUPPORTED, "measurement matrix too large");
+  const size_t want = sizeof(float) * (size_t)(B * M * S);
+  if (nbytes != want) return fail(CT_ERR_INVALID_ARGUMENT, "measurement matrix has %zu bytes, got %zu", want, nbytes);
+  std::vector<float> vpos((size_t)(3 * V));
+  std::vector<int32_t> col((size_t)V);
+  for (int64_t v = 0; v < V; ++v) {
+    for (int k = 0; k < 3; ++k) vpos[(size_t)(3 * v + k)] = desc->voxel_positions_mm[3 * cell_of[(size_t)v] + k];
+    col[(size_t)v] = (int32_t)(3 * v);
+  }
+  CT_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  TempBuffers tb;
+  float* dH = nullptr;
+  CT_CUDA(tb.get(&dH, B * M * S), "cudaMalloc");
+  rc = fill_lead_field(ctx, desc, vpos, col, dH, S);
+  if (rc) return rc;
+  CT_CUDA(cudaMemcpyAsync(out, dH, want, cudaMemcpyDeviceToHost, ctx->stream), "download");
+  CT_CUDA(cudaStreamSynchronize(ctx->stream), "download");
+  return CT_OK;
+}
+
+int ct_scenario_set_measurement_matrix(ct_scn* scn, const ct_spatial_desc* desc) {
+  if (!scn || !desc) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::vector<int64_t> cell_of;
+  int rc = check_grid(desc, cell_of);
+  if (!rc) rc = check_sensors(desc);
+  if (rc) return rc;
+  DeviceScenario& d = scn->d;
+  if ((int64_t)cell_of.size() != d.V || desc->num_sensors != d.M || desc->num_beats != d.B)
+    return fail(CT_ERR_INVALID_ARGUMENT,
+                "spatial description has %lld voxels, %lld sensors, %lld beats; the scenario %lld, %lld, %lld",
+                (long long)cell_of.size(), (long long)desc->num_sensors, (long long)desc->num_beats, (long long)d.V,
+                (long long)d.M, (long long)d.B);
+  // voxel list in device order: device voxel u is reference voxel perm[u]
+  std::vector<float> vpos((size_t)(3 * d.V));
+  std::vector<int32_t> col((size_t)d.V);
+  for (int64_t u = 0; u < d.V; ++u) {
+    const int64_t c = cell_of[(size_t)scn->perm[(size_t)u]];
+    for (int k = 0; k < 3; ++k) vpos[(size_t)(3 * u + k)] = desc->voxel_positions_mm[3 * c + k];
+    col[(size_t)u] = (int32_t)(3 * u);
+  }
+  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "scenario stream");
+  rc = fill_lead_field(scn->ctx, desc, vpos, col, d.H, d.S);
+  if (rc) return rc;
+  scn->launches += 1;
+  if (d.umma) {
+    CT_CUDA(ct::umma_prepare(d, scn->ctx->stream), "tensor-core operand split");
+    scn->launches += 2;
+  }
+  CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "measurement matrix");
+  return CT_OK;
+}
+
+int ct_delay_samples(ct_ctx* ctx, const ct_spatial_desc* desc, float* initial_delays, int32_t* delays, float* coefs,
+                     int64_t count) {
+  if (!ctx || !desc || !initial_delays || !delays || !coefs || !desc->propagation_velocities_m_per_s)
+    return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::vector<int64_t> cell_of;
+  int rc = check_grid(desc, cell_of);
+  if (rc) return rc;
+  const int64_t V = (int64_t)cell_of.size(), cells = desc->nx * desc->ny * desc->nz;
+  if (count != V * kOffsets)
+    return fail(CT_ERR_INVALID_ARGUMENT, "delay arrays have %lld elements, got %lld", (long long)(V * kOffsets),
+                (long long)count);
+  CT_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  cudaStream_t st = ctx->stream;
+  TempBuffers tb;
+  int32_t *dt = nullptr, *dn = nullptr, *dd = nullptr;
+  float *dp = nullptr, *dvel = nullptr, *ds = nullptr, *dcoef = nullptr;
+  unsigned long long* bad = nullptr;
+  CT_CUDA(tb.get(&dt, cells), "cudaMalloc");
+  CT_CUDA(tb.get(&dn, cells), "cudaMalloc");
+  CT_CUDA(tb.get(&dp, 3 * cells), "cudaMalloc");
+  CT_CUDA(tb.get(&dvel, 10), "cudaMalloc");
+  CT_CUDA(tb.get(&ds, V * kOffsets), "cudaMalloc");
+  CT_CUDA(tb.get(&dd, V * kOffsets), "cudaMalloc");
+  CT_CUDA(tb.get(&dcoef, V * kOffsets), "cudaMalloc");
+  CT_CUDA(tb.get(&bad, 1), "cudaMalloc");
+  CT_CUDA(cudaMemcpyAsync(dt, desc->voxel_types, sizeof(int32_t) * cells, cudaMemcpyHostToDevice, st), "upload");
+  CT_CUDA(cudaMemcpyAsync(dn, desc->voxel_numbers, sizeof(int32_t) * cells, cudaMemcpyHostToDevice, st), "upload");
+  CT_CUDA(cudaMemcpyAsync(dp, desc->voxel_positions_mm, sizeof(float) * 3 * cells, cudaMemcpyHostToDevice, st),
+          "upload");
+  CT_CUDA(cudaMemcpyAsync(dvel, desc->propagation_velocities_m_per_s, sizeof(float) * 10, cudaMemcpyHostToDevice, st),
+          "upload");
+  CT_CUDA(cudaMemsetAsync(bad, 0xFF, sizeof(unsigned long long), st), "memset");
+  CT_CUDA(ct::launch_delay_samples(dt, dn, dp, desc->nx, desc->ny, desc->nz, dvel, desc->sample_rate_hz, ds, dd, dcoef,
+                                   bad, ctx->num_sms, st),
+          "delay samples kernel");
+  unsigned long long first_bad = 0;
+  CT_CUDA(cudaMemcpyAsync(&first_bad, bad, sizeof(first_bad), cudaMemcpyDeviceToHost, st), "download");
+  CT_CUDA(cudaMemcpyAsync(initial_delays, ds, sizeof(float) * V * kOffsets, cudaMemcpyDeviceToHost, st), "download");
+  CT_CUDA(cudaMemcpyAsync(delays, dd, sizeof(int32_t) * V * kOffsets, cudaMemcpyDeviceToHost, st), "download");
+  CT_CUDA(cudaMemcpyAsync(coefs, dcoef, sizeof(float) * V * kOffsets, cudaMemcpyDeviceToHost, st), "download");
+  CT_CUDA(cudaStreamSynchronize(st), "delay samples");
+  if (first_bad != ~0ull) {
+    const long long c = (long long)(first_bad / kOffsets), n = (long long)(first_bad % kOffsets);
+    const long long z = c % desc->nz, y = c / desc->nz % desc->ny, x = c / (desc->ny * desc->nz);
+    return fail(CT_ERR_INVALID_ARGUMENT,
+                "can not configure delays below 1 sample (or not below 2^31): voxel (%lld, %lld, %lld), offset "
+                "column %lld",
+                x, y, z, n);
+  }
+  return CT_OK;
 }
 
 }  // extern "C"

@@ -240,6 +240,19 @@ cudaError_t launch_min_delay(DeviceScenario& d, cudaStream_t stream);
 // reference voxel of device voxel u): gather dst[u] = src[perm[u]], else scatter dst[perm[u]] = src[u].
 cudaError_t launch_permute_blocks(const void* src, void* dst, const int32_t* perm, int64_t V, int64_t words,
                                   bool gather, cudaStream_t stream);
+// Model construction (ct_model.cu). The lead-field factor of measurement.rs:85-88 for a voxel size.
+float lead_field_factor(float voxel_size_mm);
+// H[b * M + m, col[i] + a] for every beat b, sensor row m, voxel-list entry i (position vpos[i]) and
+// component a, with row pitch ldh.
+cudaError_t launch_lead_field(const float* vpos, const int32_t* col, int64_t nv, const float* spos,
+                              const float* sori, const float* off, int64_t M, int64_t B, float cf, float* H,
+                              int64_t ldh, int num_sms, cudaStream_t stream);
+// Delay samples, integer delays and coefficients [V, 26] from the voxel grid; *first_bad (preset to
+// all ones) receives the first failing cell * 26 + offset column.
+cudaError_t launch_delay_samples(const int32_t* types, const int32_t* numbers, const float* pos, int64_t nx,
+                                 int64_t ny, int64_t nz, const float* vel, float rate, float* samples,
+                                 int32_t* delays, float* coefs, unsigned long long* first_bad, int num_sms,
+                                 cudaStream_t stream);
 // Expand the deduplicated [V,78] all-pass/fir/iir state into the reference [S,78] layout.
 cudaError_t launch_expand_rows(const float* src, float* dst, int64_t V, cudaStream_t stream);
 // Last-step maximum regularisation [S] from X[T-1].

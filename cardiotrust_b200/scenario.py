@@ -465,6 +465,22 @@ def _sensors(spec: ScenarioSpec, positions: np.ndarray, mask: np.ndarray):
     return np.asarray(sp, dtype=np.float32), np.asarray(ori, dtype=np.float32)
 
 
+def array_offsets_mm(spec: ScenarioSpec) -> np.ndarray:
+    """Sensor-array offset of every beat [B, 3] (sensors.array_offsets_mm): beat b moves the array by
+    b x beat_shift_mm along x."""
+    off = np.zeros((spec.num_beats, 3), dtype=np.float32)
+    off[:, 0] = np.arange(spec.num_beats, dtype=np.float32) * np.float32(spec.beat_shift_mm)
+    return off
+
+
+def velocities_by_type(spec: ScenarioSpec) -> np.ndarray:
+    """Propagation velocity per VoxelType discriminant [10] (PropagationVelocitiesMPerS::get,
+    config/model.rs:138-150): the spec's uniform velocity for the connectable types, 0 otherwise."""
+    vel = np.zeros(10, dtype=np.float32)
+    vel[VT_SINOATRIAL:VT_PATHOLOGICAL + 1] = np.float32(spec.velocity_m_per_s)
+    return vel
+
+
 def _measurement_matrix(spec, types, numbers, positions, s_pos, s_ori) -> np.ndarray:
     """Biot-Savart lead field per beat (measurement.rs:66-123), vectorised over voxels in f32."""
     conn = numbers >= 0
@@ -478,7 +494,7 @@ def _measurement_matrix(spec, types, numbers, positions, s_pos, s_ori) -> np.nda
     cf = np.float32(np.float32(np.float32(MU0 * vol) / np.float32(4.0 * np.float32(math.pi))) * np.float32(1e12))
     H = np.zeros((B, M, S), dtype=np.float32)
     for beat in range(B):
-        offset = np.array([beat * spec.beat_shift_mm, 0.0, 0.0], dtype=np.float32)
+        offset = array_offsets_mm(spec)[beat]
         for m in range(M):
             spos = (s_pos[m] + offset).astype(np.float32)
             o = s_ori[m]

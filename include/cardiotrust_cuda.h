@@ -20,6 +20,10 @@
  *   ct_calculate_plotting_arrays <- calculate_plotting_arrays (estimations) src/core/scenario.rs:636-690
  *   ct_calculate_final    <- metrics::calculate_final     src/core/algorithm/metrics.rs:226-242
  *                            + optimal threshold summary  src/core/scenario.rs:601-617
+ *   ct_measurement_matrix <- MeasurementMatrix::from_model_spatial_description
+ *                                                         src/core/model/functional/measurement.rs:66-123
+ *   ct_delay_samples      <- calculate_delay_samples_array src/core/model/functional/allpass/delay.rs:35-111
+ *                            (+ delays/coefs of APParameters::from_model_config, allpass.rs:86-100)
  *
  * Conventions: every function returns a status (CT_OK = 0, negative CT_ERR_*),
  * never throws and never aborts. Host arrays passed in are copied; the caller
@@ -98,7 +102,7 @@ typedef struct ct_scenario_desc {
   const float* coefs;                  /* [V,26]  allpass.rs:32 */
   const int32_t* delays;               /* [V,26]  allpass.rs:33 (usize, <= 1000 after roll_delays) */
   const float* initial_delays;         /* [V,26]  allpass.rs:34 */
-  const float* measurement_matrix;     /* [B,M,S] measurement.rs:22 */
+  const float* measurement_matrix;     /* [B,M,S] measurement.rs:22; NULL = zero until ct_scenario_set_measurement_matrix */
   const float* control_matrix;         /* [S]     control.rs:23 */
   const float* control_function;       /* [T]     control.rs:142 */
   const float* measurements;           /* [B,T,M] data.simulation.measurements; may be NULL */
@@ -344,6 +348,49 @@ typedef struct ct_final_metrics {
  * or -1 (None), of the estimated model. Synchronous. */
 int ct_calculate_final(ct_scn* scn, const int32_t* ground_truth_types, const int32_t* voxel_numbers, int64_t nx,
                        int64_t ny, int64_t nz, ct_final_metrics* out);
+
+/* ---- model construction on the device (the step before the epoch) */
+
+/* The parts of the reference's SpatialDescription (src/core/model/spatial.rs) and model config that
+ * the measurement matrix and the delay arrays are built from. Arrays are C-order host arrays. */
+typedef struct ct_spatial_desc {
+  int64_t nx, ny, nz;                /* voxel grid, voxels.types.raw_dim() */
+  const int32_t* voxel_types;        /* [nx,ny,nz] VoxelType discriminants (voxels.rs:664-676); 1..6 connectable */
+  const int32_t* voxel_numbers;      /* [nx,ny,nz] state index 3v of each connectable cell's voxel, -1 = None
+                                        (voxels.numbers); the connectable cells must number 0, 3, .., S-3 once each */
+  const float* voxel_positions_mm;   /* [nx,ny,nz,3] voxels.positions_mm */
+  float voxel_size_mm;               /* voxels.size_mm */
+  float sample_rate_hz;              /* the simulation's sample rate (delay samples) */
+  const float* propagation_velocities_m_per_s; /* [10] per VoxelType discriminant (config/model.rs:138-150) */
+  int64_t num_sensors;               /* M sensor rows */
+  int64_t num_beats;                 /* B */
+  const float* sensor_positions_mm;  /* [M,3] sensors.positions_mm */
+  const float* sensor_orientations;  /* [M,3] sensors.orientations_xyz */
+  const float* sensor_array_offsets_mm; /* [B,3] sensors.array_offsets_mm */
+} ct_spatial_desc;
+
+/* MeasurementMatrix::from_model_spatial_description (src/core/model/functional/measurement.rs:66-123) on the
+ * device: the Biot-Savart lead field H [B, M, S] (S = 3 x connectable cells) in reference state order,
+ * written to the host buffer `out` of nbytes = 4 B M S. Bit-identical to the reference's f32 loop.
+ * Needs only the geometry fields and num_sensors / num_beats / sensor arrays. Synchronous. */
+int ct_measurement_matrix(ct_ctx* ctx, const ct_spatial_desc* desc, float* out, size_t nbytes);
+
+/* calculate_delay_samples_array (src/core/model/functional/allpass/delay.rs:35-111) and the integer delays
+ * and coefficients APParameters::from_model_config derives from it (allpass.rs:86-100), on the device:
+ * initial_delays (f32), delays (i32) and coefs (f32), each [V, 26] with count = V x 26 elements. Pairs
+ * whose neighbour is outside the grid or not connectable get 0 samples, delay 0 and coefficient
+ * 0.9999, as in the reference. CT_ERR_INVALID_ARGUMENT naming the first (cell, offset) in the
+ * reference's loop order whose delay is below one sample (the reference's error) or is not a finite
+ * value below 2^31 (not representable as an i32 delay). Synchronous. */
+int ct_delay_samples(ct_ctx* ctx, const ct_spatial_desc* desc, float* initial_delays, int32_t* delays, float* coefs,
+                     int64_t count);
+
+/* The measurement matrix of ct_measurement_matrix computed straight into the scenario's device copy
+ * (and its tensor-core operand splits): no [B, M, S] host array and no host-to-device copy of it.
+ * The grid's connectable cells, num_sensors and num_beats must match the scenario. A scenario may be
+ * created with measurement_matrix = NULL (H zero) and filled by this call before its first epoch.
+ * Synchronous. */
+int ct_scenario_set_measurement_matrix(ct_scn* scn, const ct_spatial_desc* desc);
 
 /* Allocation-free H x product for callers that must not see this library allocate device
  * memory: hosts that keep every device buffer in their own pool or arena or run under a fixed

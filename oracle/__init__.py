@@ -295,6 +295,54 @@ def calculate_final(system_states: np.ndarray, ground_truth_types: np.ndarray, v
     return res
 
 
+def measurement_matrix(types, numbers, positions_mm, voxel_size_mm, sensor_positions_mm, sensor_orientations,
+                       array_offsets_mm, num_states: int) -> np.ndarray:
+    """``MeasurementMatrix::from_model_spatial_description`` (src/core/model/functional/measurement.rs:66-123),
+    literal f32 loops. Returns H [B, M, S]."""
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    nums = np.ascontiguousarray(numbers, dtype=np.int32)
+    pos = np.ascontiguousarray(positions_mm, dtype=np.float32)
+    sp = np.ascontiguousarray(sensor_positions_mm, dtype=np.float32)
+    so = np.ascontiguousarray(sensor_orientations, dtype=np.float32)
+    off = np.ascontiguousarray(array_offsets_mm, dtype=np.float32).reshape(-1, 3)
+    M, B = sp.shape[0], off.shape[0]
+    H = np.zeros((B, M, num_states), np.float32)
+    fn = lib().oracle_measurement_matrix_f32
+    fn.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 3 + [ctypes.c_float] + [ctypes.c_void_p] * 3 + \
+        [ctypes.c_int64] * 3 + [ctypes.c_void_p]
+    nx, ny, nz = t.shape
+    rc = fn(t.ctypes.data, nums.ctypes.data, pos.ctypes.data, nx, ny, nz, float(voxel_size_mm), sp.ctypes.data,
+            so.ctypes.data, off.ctypes.data, M, B, num_states, H.ctypes.data)
+    if rc:
+        raise ValueError("a connectable voxel has no voxel number")
+    return H
+
+
+def delay_samples(types, numbers, positions_mm, velocities, sample_rate_hz: float, num_voxels: int):
+    """``calculate_delay_samples_array`` (src/core/model/functional/allpass/delay.rs:35-111) with the
+    integer delays and coefficients of ``APParameters::from_model_config`` (allpass.rs:86-100).
+    ``velocities``: [10] per VoxelType discriminant. Returns (samples, delays, coefs) [V, 26], or
+    raises ValueError naming the first (cell, offset column) whose delay is below one sample."""
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    nums = np.ascontiguousarray(numbers, dtype=np.int32)
+    pos = np.ascontiguousarray(positions_mm, dtype=np.float32)
+    vel = np.ascontiguousarray(velocities, dtype=np.float32)
+    samples = np.empty((num_voxels, 26), np.float32)
+    delays = np.empty((num_voxels, 26), np.int32)
+    coefs = np.empty((num_voxels, 26), np.float32)
+    fn = lib().oracle_delay_samples_f32
+    fn.restype = ctypes.c_int64
+    fn.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 3 + [ctypes.c_void_p, ctypes.c_float, ctypes.c_int64] + \
+        [ctypes.c_void_p] * 3
+    nx, ny, nz = t.shape
+    rc = fn(t.ctypes.data, nums.ctypes.data, pos.ctypes.data, nx, ny, nz, vel.ctypes.data, float(sample_rate_hz),
+            num_voxels, samples.ctypes.data, delays.ctypes.data, coefs.ctypes.data)
+    if rc:
+        cell, col = divmod(-rc - 1, 26)
+        raise ValueError(f"delay below one sample at cell {cell}, offset column {col}")
+    return samples, delays, coefs
+
+
 def algo(**kw) -> Algo:
     """An Algo with the reference defaults (config/algorithm.rs:59-85), overridden by ``kw``."""
     a = Algo()

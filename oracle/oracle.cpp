@@ -858,9 +858,100 @@ void segmentation_scores(const int32_t* pred, const int32_t* gt, int64_t cells, 
   *recall = gt_pos == 0 ? 1.0f : static_cast<float>(tp) / static_cast<float>(gt_pos);
 }
 
+// ---- model construction (the step before the epoch)
+
+// VoxelType::is_connectable (voxels.rs:690-700): Sinoatrial..Pathological = 1..6.
+bool connectable(int32_t t) { return t >= 1 && t <= 6; }
+
+// calculate_delay_s (allpass/delay.rs:14-23): |(in - out) / 1000| / velocity, f32; the norm is
+// ndarray's sum of the squared components ((0 + a) + b) + c (unrolled_fold on three elements).
+float delay_s(const float* p_in, const float* p_out, float velocity) {
+  float sq = 0.0f;
+  for (int c = 0; c < 3; ++c) {
+    const float d = (p_in[c] - p_out[c]) / 1000.0f;
+    sq = sq + d * d;
+  }
+  return std::sqrt(sq) / velocity;
+}
+
 }  // namespace
 
 extern "C" {
+
+// MeasurementMatrix::from_model_spatial_description (measurement.rs:66-123), f32, literal loops:
+// beats, then grid cells in C order (indexed_iter), connectable cells only, then sensors.
+// H [B, M, S] must be zeroed by the caller (non-connectable states stay 0 in the reference too).
+// Returns 0, or -1 when a connectable cell has no voxel number.
+int oracle_measurement_matrix_f32(const int32_t* types, const int32_t* numbers, const float* positions_mm,
+                                  int64_t nx, int64_t ny, int64_t nz, float voxel_size_mm, const float* sensor_pos,
+                                  const float* sensor_ori, const float* array_offsets, int64_t M, int64_t B, int64_t S,
+                                  float* H) {
+  const float mu0 = 1.25663706212e-6f;  // physical_constants::VACUUM_MAG_PERMEABILITY as f32
+  const float pi = 3.14159265358979323846f;  // std::f32::consts::PI
+  const float size_m = voxel_size_mm / 1000.0f;
+  const float volume = (size_m * size_m) * size_m;  // powi(3)
+  const float cf = (mu0 * volume) / (4.0f * pi) * 1e12f;
+  const int64_t cells = nx * ny * nz;
+  for (int64_t b = 0; b < B; ++b)
+    for (int64_t c = 0; c < cells; ++c) {
+      if (!connectable(types[c])) continue;
+      if (numbers[c] < 0) return -1;
+      const int64_t v = numbers[c];
+      const float* vp = positions_mm + 3 * c;
+      for (int64_t m = 0; m < M; ++m) {
+        float d[3];
+        for (int k = 0; k < 3; ++k) d[k] = ((sensor_pos[3 * m + k] + array_offsets[3 * b + k]) - vp[k]) / 1000.0f;
+        float sq = 0.0f;
+        for (int k = 0; k < 3; ++k) sq = sq + d[k] * d[k];
+        const float r = std::sqrt(sq);
+        const float r3 = (r * r) * r;
+        const float* o = sensor_ori + 3 * m;
+        float* row = H + (b * M + m) * S;
+        row[v] = cf * std::fma(o[2], d[1], -(o[1] * d[2])) / r3;
+        row[v + 1] = cf * std::fma(o[0], d[2], -(o[2] * d[0])) / r3;
+        row[v + 2] = cf * std::fma(o[1], d[0], -(o[0] * d[1])) / r3;
+      }
+    }
+  return 0;
+}
+
+// calculate_delay_samples_array (allpass/delay.rs:35-111) and the integer delays and coefficients
+// derived from it (APParameters::from_model_config, allpass.rs:86-100): for every connectable cell
+// (C order) and offset (x outer, z inner) whose neighbour is in the grid and connectable, the delay
+// in samples at the input cell's velocity (velocities indexed by VoxelType discriminant, [10]).
+// samples/delays/coefs [V, 26], zeroed/filled by this function (pairs without a neighbour: 0 samples,
+// delay 0, coefficient from_samples_to_coef(0)). Returns 0, or the first failing (cell * 26 + n) + 1
+// negated when a delay is below one sample (the reference's error), or not a finite value below 2^31.
+int64_t oracle_delay_samples_f32(const int32_t* types, const int32_t* numbers, const float* positions_mm, int64_t nx,
+                                 int64_t ny, int64_t nz, const float* velocities, float sample_rate_hz, int64_t V,
+                                 float* samples, int32_t* delays, float* coefs) {
+  for (int64_t i = 0; i < V * kOffsets; ++i) samples[i] = 0.0f;
+  for (int64_t x = 0; x < nx; ++x)
+    for (int64_t y = 0; y < ny; ++y)
+      for (int64_t z = 0; z < nz; ++z) {
+        const int64_t c = (x * ny + y) * nz + z;
+        if (!connectable(types[c])) continue;
+        int n = 0;
+        for (int ox = -1; ox <= 1; ++ox)
+          for (int oy = -1; oy <= 1; ++oy)
+            for (int oz = -1; oz <= 1; ++oz) {
+              if (ox == 0 && oy == 0 && oz == 0) continue;
+              const int col = n++;  // offset_to_delay_index (allpass.rs:578-588) in this loop order
+              const int64_t X = x + ox, Y = y + oy, Z = z + oz;
+              if (X < 0 || X >= nx || Y < 0 || Y >= ny || Z < 0 || Z >= nz) continue;
+              const int64_t co = (X * ny + Y) * nz + Z;
+              if (!connectable(types[co])) continue;
+              const float s = delay_s(positions_mm + 3 * c, positions_mm + 3 * co, velocities[types[c]]) * sample_rate_hz;
+              if (!(s >= 1.0f) || !(s < 2147483648.0f)) return -(c * kOffsets + col + 1);
+              samples[(numbers[c] / 3) * kOffsets + col] = s;
+            }
+      }
+  for (int64_t i = 0; i < V * kOffsets; ++i) {
+    delays[i] = static_cast<int32_t>(samples[i]);  // from_samples_to_usize truncates
+    coefs[i] = from_samples_to_coef_f32(samples[i]);
+  }
+  return 0;
+}
 
 // calculate_plotting_arrays, estimation side (scenario.rs:636-690 with shapes.rs:171-192,262-277,
 // 334-352). Returns 0, or -8 when a voxel's magnitude is NaN at every step (argmax_skipnan fails;
