@@ -121,6 +121,8 @@ EXPORTED = [
     "ct_measurement_matrix",
     "ct_delay_samples",
     "ct_scenario_set_measurement_matrix",
+    "ct_connect_voxels",
+    "ct_output_state_indices",
 ]
 
 PHASES = ["forward", "measure", "map_residuals", "derive", "step_metrics", "update"]
@@ -280,6 +282,8 @@ def load(path: pathlib.Path = LIB_PATH) -> ctypes.CDLL:
     lib.ct_measurement_matrix.argtypes = [vp, ctypes.POINTER(CtSpatialDesc), _fp, ctypes.c_size_t]
     lib.ct_delay_samples.argtypes = [vp, ctypes.POINTER(CtSpatialDesc), _fp, _ip, _fp, ctypes.c_int64]
     lib.ct_scenario_set_measurement_matrix.argtypes = [vp, ctypes.POINTER(CtSpatialDesc)]
+    lib.ct_connect_voxels.argtypes = [ctypes.POINTER(CtSpatialDesc), ctypes.c_float, _fp, ctypes.c_size_t, _fp]
+    lib.ct_output_state_indices.argtypes = [ctypes.POINTER(CtSpatialDesc), _ip, ctypes.c_size_t]
     for name in EXPORTED:
         getattr(lib, name)  # AttributeError if a declared symbol is not exported
     return lib

@@ -486,6 +486,35 @@ def delay_samples(ctx: Context, spatial: SpatialDescription):
     return samples, delays, coefs
 
 
+def connect_voxels(spatial: SpatialDescription, current_factor_in_pathology: float = 0.0):
+    """``connect_voxels`` (allpass.rs:295-494) in the library's native host code: (gains [S, 78],
+    activation_time_ms [nx, ny, nz], NaN where never activated)."""
+    desc, _keep = spatial.to_ct()
+    S = 3 * spatial.num_voxels
+    gains = np.empty((S, 78), np.float32)
+    act = np.empty(np.asarray(spatial.voxel_types).shape, np.float32)
+    check(lib().ct_connect_voxels(ctypes.byref(desc), float(current_factor_in_pathology), fptr(gains), gains.nbytes,
+                                  fptr(act)))
+    return gains, act
+
+
+def output_state_indices(spatial: SpatialDescription) -> np.ndarray:
+    """``init_output_state_indicies`` (allpass.rs:212-289): [S, 78] i32, -1 = None."""
+    desc, _keep = spatial.to_ct()
+    out = np.empty((3 * spatial.num_voxels, 78), np.int32)
+    check(lib().ct_output_state_indices(ctypes.byref(desc), iptr(out), out.nbytes))
+    return out
+
+
+def ap_parameters(ctx: Context, spatial: SpatialDescription, current_factor_in_pathology: float = 0.0):
+    """``APParameters::from_model_config`` (allpass.rs:71-107): gains and activation times from the
+    native activation-front search, the index table, and the delay arrays from the device."""
+    gains, act = connect_voxels(spatial, current_factor_in_pathology)
+    samples, delays, coefs = delay_samples(ctx, spatial)
+    return SimpleNamespace(gains=gains, output_state_indices=output_state_indices(spatial), coefs=coefs,
+                           delays=delays, initial_delays=samples, activation_time_ms=act)
+
+
 # ------------------------------------------------------------------------------------------
 # Reference-shaped wrappers
 

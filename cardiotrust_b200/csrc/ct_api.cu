@@ -2479,4 +2479,33 @@ int ct_delay_samples(ct_ctx* ctx, const ct_spatial_desc* desc, float* initial_de
   return CT_OK;
 }
 
+int ct_connect_voxels(const ct_spatial_desc* desc, float current_factor_in_pathology, float* gains, size_t gains_bytes,
+                      float* activation_time_ms) {
+  if (!desc || !gains || !activation_time_ms || !desc->propagation_velocities_m_per_s)
+    return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::vector<int64_t> cell_of;
+  int rc = check_grid(desc, cell_of);
+  if (rc) return rc;
+  const int64_t S = 3 * (int64_t)cell_of.size();
+  const size_t want = sizeof(float) * (size_t)(S * kGainCols);
+  if (gains_bytes != want) return fail(CT_ERR_INVALID_ARGUMENT, "gains have %zu bytes, got %zu", want, gains_bytes);
+  std::fill(gains, gains + S * kGainCols, 0.0f);
+  ct::connect_voxels_host(desc->voxel_types, desc->voxel_numbers, desc->voxel_positions_mm, desc->nx, desc->ny,
+                          desc->nz, desc->propagation_velocities_m_per_s, current_factor_in_pathology, gains,
+                          activation_time_ms);
+  return CT_OK;
+}
+
+int ct_output_state_indices(const ct_spatial_desc* desc, int32_t* out, size_t nbytes) {
+  if (!desc || !out) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::vector<int64_t> cell_of;
+  int rc = check_grid(desc, cell_of);
+  if (rc) return rc;
+  const int64_t S = 3 * (int64_t)cell_of.size();
+  const size_t want = sizeof(int32_t) * (size_t)(S * kGainCols);
+  if (nbytes != want) return fail(CT_ERR_INVALID_ARGUMENT, "output_state_indices have %zu bytes, got %zu", want, nbytes);
+  ct::output_state_indices_host(desc->voxel_types, desc->voxel_numbers, desc->nx, desc->ny, desc->nz, cell_of, out);
+  return CT_OK;
+}
+
 }  // extern "C"

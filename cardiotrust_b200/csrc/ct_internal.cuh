@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "../../include/cardiotrust_cuda.h"
 
 namespace ct {
@@ -253,6 +255,13 @@ cudaError_t launch_delay_samples(const int32_t* types, const int32_t* numbers, c
                                  int64_t ny, int64_t nz, const float* vel, float rate, float* samples,
                                  int32_t* delays, float* coefs, unsigned long long* first_bad, int num_sms,
                                  cudaStream_t stream);
+// connect_voxels (allpass.rs:295-494) on the host: gains [S,78] (zeroed by the caller) and activation
+// times in ms [cells] (NaN = never activated).
+void connect_voxels_host(const int32_t* types, const int32_t* numbers, const float* pos, int64_t nx, int64_t ny,
+                         int64_t nz, const float* vel, float factor, float* gains, float* activation_ms);
+// init_output_state_indicies (allpass.rs:212-289) on the host: [S,78], cell_of[v] = the cell of voxel v.
+void output_state_indices_host(const int32_t* types, const int32_t* numbers, int64_t nx, int64_t ny, int64_t nz,
+                               const std::vector<int64_t>& cell_of, int32_t* out);
 // Expand the deduplicated [V,78] all-pass/fir/iir state into the reference [S,78] layout.
 cudaError_t launch_expand_rows(const float* src, float* dst, int64_t V, cudaStream_t stream);
 // Last-step maximum regularisation [S] from X[T-1].

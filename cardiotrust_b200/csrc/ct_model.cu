@@ -1,15 +1,23 @@
-// Model construction on the device: the Biot-Savart measurement matrix and the all-pass delay
-// arrays, the two O(voxels x ...) fills that build a scenario before its first epoch.
+// Model construction: the Biot-Savart measurement matrix and the all-pass delay arrays on the device
+// (the two O(voxels x ...) fills that build a scenario before its first epoch), and the
+// activation-front gain search and the neighbour index table on the host.
 //
 //   lead_field_kernel    <- MeasurementMatrix::from_model_spatial_description
 //                           src/core/model/functional/measurement.rs:66-123
 //   delay_samples_kernel <- calculate_delay_samples_array src/core/model/functional/allpass/delay.rs:35-111
 //                           + from_samples_to_usize / from_samples_to_coef (allpass.rs:86-100, 644-660)
+//   connect_voxels_host  <- connect_voxels / try_to_connect src/core/model/functional/allpass.rs:295-494
+//   output_state_indices_host <- init_output_state_indicies allpass.rs:212-289
 //
 // Both are elementwise and bound by their HBM writes (12 bytes per (beat, sensor row, voxel) of H;
 // 12 bytes per (voxel, offset) of the delay arrays). Every product, sum, quotient and square root
 // is an explicitly rounded intrinsic in the reference's order, and `mul_add` is fmaf, so the
 // results equal the reference's f32 arithmetic bit for bit.
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <vector>
 
 #include "ct_internal.cuh"
 
@@ -131,6 +139,147 @@ cudaError_t launch_delay_samples(const int32_t* types, const int32_t* numbers, c
   delay_samples_kernel<<<fill_grid(n, num_sms), 256, 0, stream>>>(types, numbers, pos, nx, ny, nz, vel, rate,
                                                                    samples, delays, coefs, first_bad);
   return cudaGetLastError();
+}
+
+}  // namespace ct
+
+// ---- the activation-front search on the host (sequential by definition: a voxel's gains depend on
+// which neighbour reached it first)
+
+namespace ct {
+namespace {
+
+// approx::relative_eq! with epsilon = max_relative = f32::EPSILON.
+bool relative_eq(float a, float b) {
+  if (a == b) return true;
+  if (std::isinf(a) || std::isinf(b)) return false;
+  const float eps = 1.1920929e-7f;
+  const float diff = std::fabs(a - b);
+  return diff <= eps || diff <= std::fmax(std::fabs(a), std::fabs(b)) * eps;
+}
+
+bool host_connectable(int32_t t) { return t >= 1 && t <= 6; }
+
+// voxels::is_connection_allowed(output, input), voxels.rs:707-742 (bit i of the mask: input type i).
+bool allowed(int32_t out, int32_t in) {
+  static const unsigned mask[10] = {0u,
+                                    (1u << 2) | (1u << 5) | (1u << 6),
+                                    (1u << 1) | (1u << 2) | (1u << 3) | (1u << 6),
+                                    (1u << 2) | (1u << 4) | (1u << 6),
+                                    (1u << 3) | (1u << 4) | (1u << 5) | (1u << 6),
+                                    (1u << 4) | (1u << 5) | (1u << 6),
+                                    0x3FFu,
+                                    0u,
+                                    0u,
+                                    0u};
+  if (out < 0 || out > 9 || in < 0 || in > 9) return false;
+  return (mask[out] >> in) & 1u;
+}
+
+}  // namespace
+
+// connect_voxels / try_to_connect (allpass.rs:295-494) with the reference's exact visiting rule:
+// `current` runs through 0 and then each next larger activation time; at each, the voxels whose time
+// is relative_eq to it (C order, a snapshot) try their 26 offsets (x outer, z inner), each activating
+// an allowed, not yet activated input first come, first served. The activation times live in an
+// ordered map, so a sweep step touches only the voxels near `current` instead of the whole grid.
+// Voxel numbers must be valid for every connectable cell (checked by the caller).
+void connect_voxels_host(const int32_t* types, const int32_t* numbers, const float* pos, int64_t nx, int64_t ny,
+                         int64_t nz, const float* vel, float factor, float* gains, float* activation_ms) {
+  const int64_t cells = nx * ny * nz;
+  const float nan = std::nanf("");
+  std::vector<float> t((size_t)cells, nan);
+  std::vector<float> dir((size_t)(3 * cells), 0.0f);
+  std::map<float, std::vector<int64_t>> by_time;
+  for (int64_t c = 0; c < cells; ++c)
+    if (types[c] == 1) {  // Sinoatrial
+      t[(size_t)c] = 0.0f;
+      dir[(size_t)(3 * c)] = 1.0f;
+      by_time[0.0f].push_back(c);
+    }
+  const bool skip_patho = relative_eq(factor, 0.0f);
+  const float inv = 1.0f / factor;
+  float current = 0.0f;
+  std::vector<int64_t> cand;
+  for (;;) {
+    // the times relative_eq to `current` lie within 2 max(eps, |current| eps) of it
+    const float w = 2.0f * std::fmax(1.1920929e-7f, std::fabs(current) * 1.1920929e-7f);
+    cand.clear();
+    for (auto it = by_time.lower_bound(current - w); it != by_time.end() && it->first <= current + w; ++it)
+      if (relative_eq(it->first, current)) cand.insert(cand.end(), it->second.begin(), it->second.end());
+    std::sort(cand.begin(), cand.end());
+    for (int64_t out : cand) {
+      const int64_t xo = out / (ny * nz), yo = out / nz % ny, zo = out % nz;
+      const int32_t type_out = types[out];
+      for (int ox = -1; ox <= 1; ++ox)
+        for (int oy = -1; oy <= 1; ++oy)
+          for (int oz = -1; oz <= 1; ++oz) {
+            if (ox == 0 && oy == 0 && oz == 0) continue;
+            const int64_t xi = xo - ox, yi = yo - oy, zi = zo - oz;
+            if (xi < 0 || xi >= nx || yi < 0 || yi >= ny || zi < 0 || zi >= nz) continue;
+            const int64_t in = (xi * ny + yi) * nz + zi;
+            const int32_t type_in = types[in];
+            if (!host_connectable(type_in) || !std::isnan(t[(size_t)in])) continue;
+            if (!allowed(type_out, type_in)) continue;
+            if (type_in == 6 && skip_patho) continue;
+            const float* pin = pos + 3 * in;
+            const float* pout = pos + 3 * out;
+            float d[3], sq = 0.0f, norm = 0.0f;
+            for (int k = 0; k < 3; ++k) {
+              d[k] = (pin[k] - pout[k]) / 1000.0f;
+              sq = sq + d[k] * d[k];
+              norm = norm + std::fabs(d[k]);
+            }
+            const float ti = t[(size_t)out] + std::sqrt(sq) / vel[type_in];  // calculate_delay_s
+            t[(size_t)in] = ti;
+            by_time[ti].push_back(in);
+            for (int k = 0; k < 3; ++k) dir[(size_t)(3 * in + k)] = d[k] / norm;  // direction::calculate
+            int k0 = (oz + 1) * 3 + (oy + 1) * 9 + (ox + 1) * 27;  // offset_to_gain_index, output dim 0
+            if (k0 > 27 + 9 + 3) k0 -= 3;
+            for (int i = 0; i < 3; ++i)
+              for (int o = 0; o < 3; ++o) {
+                const float c = dir[(size_t)(3 * out + o)];
+                const float mult = relative_eq(c, 0.0f) ? 0.0f : (c > 0.0f ? 1.0f : -1.0f);
+                float g = dir[(size_t)(3 * in + i)] * mult;  // gain::calculate
+                if (type_in == 6 && type_out != 6) g = g * factor;
+                if (type_out == 6 && type_in != 6) g = g * inv;
+                gains[((int64_t)numbers[in] + i) * kGainCols + k0 + o] = g;
+              }
+          }
+    }
+    auto next = by_time.upper_bound(current);
+    // no later activation time: the reference's next sweep step finds no voxel and ends the loop
+    if (next == by_time.end()) break;
+    current = next->first;
+  }
+  for (int64_t c = 0; c < cells; ++c) activation_ms[c] = t[(size_t)c] * 1000.0f;
+}
+
+// init_output_state_indicies (allpass.rs:212-289): row 3v + a, column 3n + b holds 3 w + b for the
+// voxel w at offset n of voxel v (in the grid and connectable), -1 otherwise. `cell_of[v]` = the cell
+// of voxel v.
+void output_state_indices_host(const int32_t* types, const int32_t* numbers, int64_t nx, int64_t ny, int64_t nz,
+                               const std::vector<int64_t>& cell_of, int32_t* out) {
+  const int64_t V = (int64_t)cell_of.size();
+  for (int64_t v = 0; v < V; ++v) {
+    const int64_t c = cell_of[(size_t)v];
+    const int64_t x = c / (ny * nz), y = c / nz % ny, z = c % nz;
+    int n = 0;
+    for (int ox = -1; ox <= 1; ++ox)
+      for (int oy = -1; oy <= 1; ++oy)
+        for (int oz = -1; oz <= 1; ++oz) {
+          if (ox == 0 && oy == 0 && oz == 0) continue;
+          const int col = n++;
+          const int64_t X = x + ox, Y = y + oy, Z = z + oz;
+          int32_t w = -1;
+          if (X >= 0 && X < nx && Y >= 0 && Y < ny && Z >= 0 && Z < nz) {
+            const int64_t co = (X * ny + Y) * nz + Z;
+            if (host_connectable(types[co])) w = numbers[co];
+          }
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) out[(3 * v + a) * kGainCols + 3 * col + b] = w < 0 ? -1 : w + b;
+        }
+  }
 }
 
 }  // namespace ct

@@ -24,6 +24,8 @@
  *                                                         src/core/model/functional/measurement.rs:66-123
  *   ct_delay_samples      <- calculate_delay_samples_array src/core/model/functional/allpass/delay.rs:35-111
  *                            (+ delays/coefs of APParameters::from_model_config, allpass.rs:86-100)
+ *   ct_connect_voxels     <- connect_voxels               src/core/model/functional/allpass.rs:295-494
+ *   ct_output_state_indices <- init_output_state_indicies src/core/model/functional/allpass.rs:212-289
  *
  * Conventions: every function returns a status (CT_OK = 0, negative CT_ERR_*),
  * never throws and never aborts. Host arrays passed in are copied; the caller
@@ -391,6 +393,23 @@ int ct_delay_samples(ct_ctx* ctx, const ct_spatial_desc* desc, float* initial_de
  * created with measurement_matrix = NULL (H zero) and filled by this call before its first epoch.
  * Synchronous. */
 int ct_scenario_set_measurement_matrix(ct_scn* scn, const ct_spatial_desc* desc);
+
+/* connect_voxels / try_to_connect (src/core/model/functional/allpass.rs:295-494): the activation-front
+ * search that sets the gains. Starting from the Sinoatrial voxels at time 0 it visits activation times
+ * in increasing order; the voxels whose time is relative_eq to the current one (C order) each activate
+ * their allowed (voxels.rs:707-742), not yet activated neighbours first come, first served, at the
+ * input's velocity; the input's current direction is (in - out) / |in - out|_1 and its gains
+ * gain::calculate (gain.rs:9-29) times the pathology factor (or its inverse). Writes gains [S, 78]
+ * (gains_bytes = 4 S 78) and activation_time_ms [nx, ny, nz] (NaN = never activated), bit-identical
+ * to the reference's f32 loop. Host-only (sequential by definition: a voxel's gains depend on which
+ * neighbour reached it first); needs the grid fields and the velocities. Synchronous. */
+int ct_connect_voxels(const ct_spatial_desc* desc, float current_factor_in_pathology, float* gains, size_t gains_bytes,
+                      float* activation_time_ms);
+
+/* init_output_state_indicies (src/core/model/functional/allpass.rs:212-289): [S, 78] i32, row 3v + a,
+ * column 3n + b = 3w + b for the voxel w at offset n of voxel v, -1 where there is none
+ * (nbytes = 4 S 78). Host-only. */
+int ct_output_state_indices(const ct_spatial_desc* desc, int32_t* out, size_t nbytes);
 
 /* Allocation-free H x product for callers that must not see this library allocate device
  * memory: hosts that keep every device buffer in their own pool or arena or run under a fixed

@@ -318,6 +318,26 @@ def measurement_matrix(types, numbers, positions_mm, voxel_size_mm, sensor_posit
     return H
 
 
+def connect_voxels(types, numbers, positions_mm, velocities, current_factor_in_pathology: float, num_states: int):
+    """``connect_voxels`` / ``try_to_connect`` (src/core/model/functional/allpass.rs:295-494), the literal
+    activation-time sweep (small grids: O(activation times x cells)). Returns (gains [S, 78],
+    activation_time_ms [nx, ny, nz], NaN where never activated)."""
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    nums = np.ascontiguousarray(numbers, dtype=np.int32)
+    pos = np.ascontiguousarray(positions_mm, dtype=np.float32)
+    vel = np.ascontiguousarray(velocities, dtype=np.float32)
+    gains = np.zeros((num_states, 78), np.float32)
+    act = np.empty(t.shape, np.float32)
+    fn = lib().oracle_connect_voxels_f32
+    fn.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 3 + [ctypes.c_void_p, ctypes.c_float] + \
+        [ctypes.c_void_p] * 2
+    nx, ny, nz = t.shape
+    if fn(t.ctypes.data, nums.ctypes.data, pos.ctypes.data, nx, ny, nz, vel.ctypes.data,
+          float(current_factor_in_pathology), gains.ctypes.data, act.ctypes.data):
+        raise ValueError("an activated voxel has no voxel number")
+    return gains, act
+
+
 def delay_samples(types, numbers, positions_mm, velocities, sample_rate_hz: float, num_voxels: int):
     """``calculate_delay_samples_array`` (src/core/model/functional/allpass/delay.rs:35-111) with the
     integer delays and coefficients of ``APParameters::from_model_config`` (allpass.rs:86-100).

@@ -874,9 +874,120 @@ float delay_s(const float* p_in, const float* p_out, float velocity) {
   return std::sqrt(sq) / velocity;
 }
 
+// approx::relative_eq! with the defaults epsilon = max_relative = f32::EPSILON.
+bool relative_eq_f32(float a, float b) {
+  if (a == b) return true;
+  if (std::isinf(a) || std::isinf(b)) return false;
+  const float eps = 1.1920929e-7f;
+  const float diff = std::fabs(a - b);
+  if (diff <= eps) return true;
+  return diff <= std::fmax(std::fabs(a), std::fabs(b)) * eps;
+}
+
+// voxels::is_connection_allowed(output, input) (voxels.rs:707-742); discriminants voxels.rs:664-676.
+bool connection_allowed(int32_t out, int32_t in) {
+  switch (out) {
+    case 1: return in == 2 || in == 6 || in == 5;            // Sinoatrial <- Atrium, Pathological, Ventricle
+    case 2: return in == 1 || in == 2 || in == 3 || in == 6;  // Atrium <- SA, Atrium, AV, Pathological
+    case 3: return in == 2 || in == 4 || in == 6;             // AV <- Atrium, HPS, Pathological
+    case 4: return in == 4 || in == 3 || in == 5 || in == 6;  // HPS <- HPS, AV, Ventricle, Pathological
+    case 5: return in == 5 || in == 4 || in == 6;             // Ventricle <- Ventricle, HPS, Pathological
+    case 6: return true;                                      // Pathological
+    default: return false;                                    // None, Vessel, Torso, Chamber
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+// connect_voxels / try_to_connect (allpass.rs:295-494), literal: the activation-time sweep visits
+// `current` = 0, then the smallest activation time above it, and so on; at each, every voxel whose
+// time is relative_eq to `current` (a snapshot, C order) tries the 26 offsets (x outer, z inner) and
+// activates each allowed, not yet activated input voxel (first come, first served) with
+// time(out) + delay at the input's velocity, the direction (in - out) / |in - out|_1, and the gains
+// gain::calculate (gain.rs:9-29) x the pathology factors. O(times x cells): small grids only.
+// gains [S, 78] zeroed by the caller; activation_ms [cells] (NaN = None). Returns 0, or -1 when an
+// activated cell has no voxel number.
+int oracle_connect_voxels_f32(const int32_t* types, const int32_t* numbers, const float* positions_mm, int64_t nx,
+                              int64_t ny, int64_t nz, const float* velocities, float current_factor_in_pathology,
+                              float* gains, float* activation_ms) {
+  const int64_t cells = nx * ny * nz;
+  const float nan = std::nanf("");
+  std::vector<float> t((size_t)cells, nan);
+  std::vector<float> dir((size_t)(3 * cells), 0.0f);
+  for (int64_t c = 0; c < cells; ++c)
+    if (types[c] == 1) {
+      t[(size_t)c] = 0.0f;
+      dir[(size_t)(3 * c)] = 1.0f;
+    }
+  float current = 0.0f;
+  bool connected = true;
+  while (connected) {
+    bool future = false;
+    for (float v : t)
+      if (!std::isnan(v) && v > current) future = true;
+    if (!future) connected = false;
+    std::vector<int64_t> cand;
+    for (int64_t c = 0; c < cells; ++c)
+      if (!std::isnan(t[(size_t)c]) && relative_eq_f32(t[(size_t)c], current)) cand.push_back(c);
+    for (int64_t out : cand) {
+      const int64_t xo = out / (ny * nz), yo = out / nz % ny, zo = out % nz;
+      for (int ox = -1; ox <= 1; ++ox)
+        for (int oy = -1; oy <= 1; ++oy)
+          for (int oz = -1; oz <= 1; ++oz) {
+            if (ox == 0 && oy == 0 && oz == 0) continue;
+            const int64_t xi = xo - ox, yi = yo - oy, zi = zo - oz;
+            if (xi < 0 || xi >= nx || yi < 0 || yi >= ny || zi < 0 || zi >= nz) continue;
+            const int64_t in = (xi * ny + yi) * nz + zi;
+            if (!connectable(types[in])) continue;  // is_valid_index
+            if (!std::isnan(t[(size_t)in])) continue;
+            if (!connection_allowed(types[out], types[in])) continue;
+            if (types[in] == 6 && relative_eq_f32(current_factor_in_pathology, 0.0f)) continue;
+            if (numbers[in] < 0) return -1;
+            const float* pin = positions_mm + 3 * in;
+            const float* pout = positions_mm + 3 * out;
+            t[(size_t)in] = t[(size_t)out] + delay_s(pin, pout, velocities[types[in]]);
+            // direction::calculate (direction.rs:13-22)
+            float d[3], norm = 0.0f;
+            for (int k = 0; k < 3; ++k) {
+              d[k] = (pin[k] - pout[k]) / 1000.0f;
+              norm = norm + std::fabs(d[k]);
+            }
+            for (int k = 0; k < 3; ++k) dir[(size_t)(3 * in + k)] = d[k] / norm;
+            float g[3][3];
+            for (int i = 0; i < 3; ++i)
+              for (int o = 0; o < 3; ++o) {
+                const float c = dir[(size_t)(3 * out + o)];
+                const float mult = relative_eq_f32(c, 0.0f) ? 0.0f : (c > 0.0f ? 1.0f : (c < 0.0f ? -1.0f : c));
+                g[i][o] = dir[(size_t)(3 * in + i)] * mult;
+              }
+            if (types[in] == 6 && types[out] != 6)
+              for (auto& row : g)
+                for (float& v : row) v = v * current_factor_in_pathology;
+            if (types[out] == 6 && types[in] != 6) {
+              const float inv = 1.0f / current_factor_in_pathology;
+              for (auto& row : g)
+                for (float& v : row) v = v * inv;
+            }
+            // assign_gain (allpass.rs:501-523) with offset_to_gain_index (allpass.rs:532-548)
+            for (int i = 0; i < 3; ++i)
+              for (int o = 0; o < 3; ++o) {
+                int k = o + (oz + 1) * 3 + (oy + 1) * 9 + (ox + 1) * 27;
+                if (k > 27 + 9 + 3) k -= 3;
+                gains[((int64_t)numbers[in] + i) * kGainCols + k] = g[i][o];
+              }
+            connected = true;
+          }
+    }
+    float next = nan;
+    for (float v : t)
+      if (!std::isnan(v) && v > current && (std::isnan(next) || v < next)) next = v;
+    current = next;  // min_skipnan of the times above `current` (NaN when there are none)
+  }
+  for (int64_t c = 0; c < cells; ++c) activation_ms[c] = t[(size_t)c] * 1000.0f;
+  return 0;
+}
 
 // MeasurementMatrix::from_model_spatial_description (measurement.rs:66-123), f32, literal loops:
 // beats, then grid cells in C order (indexed_iter), connectable cells only, then sensors.
