@@ -373,7 +373,7 @@ def _noisy_scenario(alg, sc, ctx, spec):
     """A batch-workload scenario with its ground truth from the CUDA forward plus the spec's noise."""
     import numpy as np
 
-    scn = sc.build(spec)
+    scn = sc.build(spec, ctx=ctx)
     truth = alg.EpochEngine.from_scenario(ctx, scn, truth=True)
     y = truth.simulate()
     truth.close()
@@ -619,7 +619,7 @@ def gpu_arm(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx = alg.Context(local_rank, stream=stream.cuda_stream)
-    scn = sc.build(sc.workload_spec(args.workload, seed=rank))
+    scn = sc.build(sc.workload_spec(args.workload, seed=rank), ctx=ctx)
     # ground truth with the CUDA forward (Simulation::run reuses the prediction path)
     truth = alg.EpochEngine.from_scenario(ctx, scn, truth=True)
     y = truth.simulate()

@@ -521,8 +521,12 @@ def _pulse(num_steps: int, sigma: float, onset: int) -> np.ndarray:
     return u.astype(np.float32)
 
 
-def build(spec: ScenarioSpec) -> Scenario:
-    """Build a scenario (everything except the ground-truth measurements)."""
+def build(spec: ScenarioSpec, ctx=None) -> Scenario:
+    """Build a scenario (everything except the ground-truth measurements).
+
+    With ``ctx`` (an ``algorithm.Context``) the model arrays come from the library: the
+    activation-front gain search and the index table in its native host code, the delay arrays and
+    the measurement matrix on the device (bit-identical to the numpy restatement used otherwise)."""
     rng = np.random.default_rng(spec.seed)
     mask = _mask(spec)
     nx, ny, nz = spec.shape
@@ -554,11 +558,28 @@ def build(spec: ScenarioSpec) -> Scenario:
 
     numbers = _numbers(types_model)
     positions = _positions(spec.shape, spec.voxel_size_mm)
-    model = _ap_params(types_model, numbers, positions, spec, current_factor=0.0)
-    truth = _ap_params(types_truth, numbers, positions, spec, current_factor=0.0)
-
     s_pos, s_ori = _sensors(spec, positions, mask)
-    H = _measurement_matrix(spec, types_model, numbers, positions, s_pos, s_ori)
+    if ctx is None:
+        model = _ap_params(types_model, numbers, positions, spec, current_factor=0.0)
+        truth = _ap_params(types_truth, numbers, positions, spec, current_factor=0.0)
+        H = _measurement_matrix(spec, types_model, numbers, positions, s_pos, s_ori)
+    else:
+        from . import algorithm as alg
+
+        def spatial(types):
+            return alg.SpatialDescription(voxel_types=types, voxel_numbers=numbers, voxel_positions_mm=positions,
+                                          voxel_size_mm=spec.voxel_size_mm, sensor_positions_mm=s_pos,
+                                          sensor_orientations=s_ori, sensor_array_offsets_mm=array_offsets_mm(spec),
+                                          sample_rate_hz=spec.sample_rate_hz,
+                                          propagation_velocities_m_per_s=velocities_by_type(spec))
+
+        def params(types):
+            p = alg.ap_parameters(ctx, spatial(types), 0.0)
+            return APParams(gains=p.gains, output_state_indices=p.output_state_indices, coefs=p.coefs,
+                            delays=p.delays, initial_delays=p.initial_delays, activation_time_ms=p.activation_time_ms)
+
+        model, truth = params(types_model), params(types_truth)
+        H = alg.measurement_matrix(ctx, spatial(types_model))
 
     S = 3 * model.coefs.shape[0]
     control_matrix = np.zeros(S, dtype=np.float32)

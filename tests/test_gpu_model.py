@@ -163,3 +163,19 @@ def test_scenario_lead_field_on_device_gives_identical_epochs(alg, ctx, oracle_m
             dev.set_measurement_matrix(sd)
         host.close()
         dev.close()
+
+
+@pytest.mark.parametrize("name", ["cuboid8_b2", "shell_b3"])
+def test_builder_on_the_library_equals_numpy_builder(alg, ctx, name):
+    """scenario.build(spec, ctx): gains, index table and activation times from the native search, delay
+    arrays and measurement matrix from the device - the same scenario as the numpy restatement."""
+    from cardiotrust_b200 import scenario as sc
+
+    spec = _specs()[name]
+    a, b = sc.build(spec), sc.build(spec, ctx=ctx)
+    assert np.array_equal(a.measurement_matrix, b.measurement_matrix)
+    for p, q in ((a.model, b.model), (a.truth, b.truth)):
+        for f in ("gains", "output_state_indices", "coefs", "delays", "initial_delays", "activation_time_ms"):
+            x, y = getattr(p, f), getattr(q, f)
+            assert x.dtype == y.dtype and x.shape == y.shape, f
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), f
