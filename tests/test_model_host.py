@@ -129,3 +129,48 @@ def test_invalid_numbering_and_sizes_are_rejected(alg):
 
     assert lib().ct_connect_voxels(ctypes.byref(desc), 0.0, fptr(small), small.nbytes, fptr(act)) == \
         CT_ERR_INVALID_ARGUMENT
+
+
+def test_no_sinoatrial_voxel_activates_nothing(alg, oracle_mod):
+    """Without a Sinoatrial voxel the reference's sweep finds no candidate at time 0 and stops: every
+    activation time stays None and every gain 0."""
+    s = sc.build(SPECS["cuboid8"])
+    sd = alg.SpatialDescription.from_scenario(s)
+    types = sd.voxel_types.copy()
+    types[types == sc.VT_SINOATRIAL] = sc.VT_VENTRICLE
+    sd.voxel_types = types
+    gains, act = alg.connect_voxels(sd, 0.0)
+    g_o, a_o = _oracle(oracle_mod, sd, 0.0)
+    assert np.all(np.isnan(act)) and np.all(np.isnan(a_o))
+    assert not gains.any() and not g_o.any()
+
+
+def test_isolated_voxel_and_unknown_types(alg, oracle_mod):
+    """A connectable voxel with no connectable neighbour is never activated; cells of non-connectable
+    types (Vessel, Torso, Chamber) neither carry voxels nor pass the front."""
+    types = np.full((6, 5, 4), sc.VT_VENTRICLE, np.int32)
+    types[0, 0, 0] = sc.VT_SINOATRIAL
+    types[3, :, :] = sc.VT_TORSO  # a wall the front cannot cross
+    types[5, 4, 3] = sc.VT_VENTRICLE
+    types[4, :, :] = sc.VT_CHAMBER
+    types[5, :, :] = sc.VT_VESSEL
+    types[5, 4, 3] = sc.VT_VENTRICLE  # isolated behind the wall
+    numbers = np.full(types.shape, -1, np.int32)
+    conn = (types >= 1) & (types <= 6)
+    numbers[conn] = 3 * np.arange(int(conn.sum()), dtype=np.int32)
+    pos = (np.stack(np.meshgrid(*[np.arange(n) for n in types.shape], indexing="ij"), axis=-1) * 2.5).astype(np.float32)
+    vel = np.zeros(10, np.float32)
+    vel[1:7] = 0.6
+    sd = alg.SpatialDescription(voxel_types=types, voxel_numbers=numbers, voxel_positions_mm=pos, voxel_size_mm=2.5,
+                                sensor_positions_mm=np.zeros((3, 3), np.float32),
+                                sensor_orientations=np.eye(3, dtype=np.float32),
+                                sensor_array_offsets_mm=np.zeros((1, 3), np.float32),
+                                propagation_velocities_m_per_s=vel)
+    gains, act = alg.connect_voxels(sd, 0.0)
+    g_o, a_o = _oracle(oracle_mod, sd, 0.0)
+    assert _same(gains, g_o) and _same(act, a_o)
+    assert np.all(np.isfinite(act[:3])) and np.all(np.isnan(act[3:]))
+    v_iso = numbers[5, 4, 3] // 3
+    assert not gains[3 * v_iso:3 * v_iso + 3].any()
+    osi = alg.output_state_indices(sd)
+    assert np.all(osi[3 * v_iso:3 * v_iso + 3] == -1)  # no connectable neighbour at any offset
