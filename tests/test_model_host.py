@@ -174,3 +174,27 @@ def test_isolated_voxel_and_unknown_types(alg, oracle_mod):
     assert not gains[3 * v_iso:3 * v_iso + 3].any()
     osi = alg.output_state_indices(sd)
     assert np.all(osi[3 * v_iso:3 * v_iso + 3] == -1)  # no connectable neighbour at any offset
+
+
+def test_spatial_description_shapes_are_checked(alg):
+    """The Python mirror refuses malformed arrays before any library call."""
+    from cardiotrust_b200._lib import CtError
+
+    s = sc.build(SPECS["cuboid8"])
+    good = alg.SpatialDescription.from_scenario(s)
+    assert good.num_voxels == s.num_voxels and good.num_sensors == s.num_sensors and good.num_beats == 1
+    for field, value in (("voxel_numbers", s.numbers[:-1]), ("voxel_positions_mm", s.positions_mm[..., :2]),
+                         ("sensor_orientations", s.sensor_orientations[:-1]),
+                         ("propagation_velocities_m_per_s", np.zeros(6, np.float32))):
+        bad = alg.SpatialDescription.from_scenario(s)
+        setattr(bad, field, value)
+        with pytest.raises(CtError):
+            bad.to_ct()
+
+
+def test_array_offsets_and_velocities(alg):
+    spec = sc.ScenarioSpec(shape=(4, 4, 4), num_beats=3, beat_shift_mm=7.5, velocity_m_per_s=0.8)
+    off = sc.array_offsets_mm(spec)
+    assert off.shape == (3, 3) and np.array_equal(off[:, 0], np.float32([0.0, 7.5, 15.0])) and not off[:, 1:].any()
+    vel = sc.velocities_by_type(spec)
+    assert vel.shape == (10,) and np.all(vel[1:7] == np.float32(0.8)) and vel[0] == 0 and not vel[7:].any()
