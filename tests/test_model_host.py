@@ -198,3 +198,14 @@ def test_array_offsets_and_velocities(alg):
     assert off.shape == (3, 3) and np.array_equal(off[:, 0], np.float32([0.0, 7.5, 15.0])) and not off[:, 1:].any()
     vel = sc.velocities_by_type(spec)
     assert vel.shape == (10,) and np.all(vel[1:7] == np.float32(0.8)) and vel[0] == 0 and not vel[7:].any()
+
+
+def test_full_size_shell_matches_literal_sweep(alg, oracle_mod):
+    """The 64x64x48 ellipsoidal shell of the adjoint and precision configs (47,264 voxels): the native
+    search equals the literal sweep (a full grid scan per activation time, ~10 s) bit for bit."""
+    s = sc.build(sc.workload_spec("shell"))
+    sd = alg.SpatialDescription.from_scenario(s)
+    gains, act = alg.connect_voxels(sd, 0.0)
+    g_o, a_o = _oracle(oracle_mod, sd, 0.0)
+    assert _same(gains, g_o) and _same(act, a_o)
+    assert np.isfinite(act).sum() == sd.num_voxels
