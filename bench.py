@@ -47,7 +47,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--cpu-steps", type=int, default=200, help="steps of the bounded CPU sample")
-    p.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "tf32"],
+    p.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "tf32", "bf16x6"],
                    help="measurement products: FP32 CUDA cores, tcgen05 split TF32, tcgen05 TF32")
     p.add_argument("--batch-scenarios", type=int, default=64,
                    help="scenarios of the batched section (0 skips it)")
@@ -485,7 +485,7 @@ def batched_section(args, alg, sc, ctx, prec, stream, flush):
         "build_s": build_s,
         "chosen": {"form": "batched: one persistent forward and one persistent adjoint launch per beat index over "
                            "every member's tiles, epoch replayed from a CUDA graph; adjoint gradients, checkpoint interval "
-                           "from the autotuner", "precision": f"{['fp32', 'tf32x3', 'tf32'][int(prec)]} products for every member",
+                           "from the autotuner", "precision": f"{['fp32', 'tf32x3', 'tf32', 'bf16x6'][int(prec)]} products for every member",
                    "scenario_epochs_per_s": chosen, "voxel_steps_per_s": vtb * 1000.0 / chosen_ms,
                    "ms_per_epoch": chosen_ms, "graph_kernels": info["graph_kernels"], "uses_graph": info["uses_graph"],
                    "forward_ctas": info["forward_ctas"], "adjoint_ctas": info["adjoint_ctas"], "autotuned": tuned,
@@ -566,7 +566,8 @@ def precision_case(alg, ctx, scn, ref):
         return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
     results = {}
-    for name, prec in (("fp32", alg.Precision.Fp32), ("tf32x3", alg.Precision.Tf32x3), ("tf32", alg.Precision.Tf32)):
+    for name, prec in (("fp32", alg.Precision.Fp32), ("tf32x3", alg.Precision.Tf32x3), ("tf32", alg.Precision.Tf32),
+                       ("bf16x6", alg.Precision.Bf16x6)):
         eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=cfg)
         eng.run_epoch(0, beat_order=np.arange(scn.num_beats), precision=prec)
         r = {f: rel(eng.read(f), ref[f]) for f in ("system_states", "measurements", "residuals", "grad_gains",
@@ -629,7 +630,8 @@ def gpu_arm(args):
     scn.measurements = (y + rng.normal(0.0, sigma, size=y.shape)).astype(np.float32)
 
     cfg = algorithm_config(alg)
-    prec = {"fp32": alg.Precision.Fp32, "tf32x3": alg.Precision.Tf32x3, "tf32": alg.Precision.Tf32}[args.precision]
+    prec = {"fp32": alg.Precision.Fp32, "tf32x3": alg.Precision.Tf32x3, "tf32": alg.Precision.Tf32,
+            "bf16x6": alg.Precision.Bf16x6}[args.precision]
     total_epochs = args.warmup + 3 * args.steps + 4
     eng = alg.EpochEngine.from_scenario(ctx, scn, num_batch_slots=total_epochs, algorithm=cfg)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2

@@ -31,6 +31,7 @@ CT_GRAD_REFERENCE = 0
 CT_PREC_FP32 = 0
 CT_PREC_TF32X3 = 1
 CT_PREC_TF32 = 2
+CT_PREC_BF16X6 = 3
 
 # ct_field values with (dtype, shape-builder(S, V, M, T, B, NB))
 FIELDS = {

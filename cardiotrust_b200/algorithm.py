@@ -46,6 +46,7 @@ class Precision(enum.IntEnum):
     Fp32 = 0  # FP32 CUDA-core GEMMs
     Tf32x3 = 1  # tcgen05 TF32 with hi/lo operand split
     Tf32 = 2  # tcgen05 TF32, one pass
+    Bf16x6 = 3  # tcgen05 BF16 on error-free 8-bit slices, exact accumulation (unbiased like FP32)
 
 
 @dataclasses.dataclass

@@ -19,8 +19,8 @@ LIB = PKG / "libcardiotrust_cuda.so"
 BUILD_DIR = PKG / "_build"
 
 SOURCES = ["ct_api.cu", "ct_propagate.cu", "ct_measure.cu", "ct_derive.cu", "ct_update.cu", "ct_umma.cu", "ct_adjoint.cu", "ct_plain.cu",
-           "ct_post.cu", "ct_model.cu"]
-HEADERS = ["ct_internal.cuh", "ct_sync.cuh"]
+           "ct_post.cu", "ct_model.cu", "ct_slice.cu"]
+HEADERS = ["ct_internal.cuh", "ct_sync.cuh", "ct_tcgen05.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -115,6 +115,29 @@ int cuda_fail(cudaError_t err, const char* what) {
     if (err__ != cudaSuccess) return cuda_fail(err__, what); \
   } while (0)
 
+// Makes `device` current for the rest of the enclosing scope and restores the caller's current
+// device when the scope ends, so that no entry point changes the calling thread's device.
+struct DeviceScope {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit DeviceScope(int device) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+    if (prev != device) err = cudaSetDevice(device);
+  }
+  ~DeviceScope() {
+    int now = -1;
+    if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+  }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+};
+#define CT_DEVICE_SCOPE(device)           \
+  DeviceScope device_scope__(device);     \
+  CT_CUDA(device_scope__.err, "cudaSetDevice")
+
 cudaEvent_t take_event(ct_scn* s) {
   if (!s->event_pool.empty()) {
     cudaEvent_t e = s->event_pool.back();
@@ -227,6 +250,45 @@ void refresh_delay_bound(ct_scn* s) {
   s->updates_at_read = -1;
 }
 
+bool valid_precision(int p) {
+  return p == CT_PREC_FP32 || p == CT_PREC_TF32X3 || p == CT_PREC_TF32 || p == CT_PREC_BF16X6;
+}
+
+// Sliced BF16 operands (ct_slice.cu): buffers allocated on first use, H and H^T sliced once per
+// measurement matrix. Synchronous when it slices (the temporary buffer of the transpose).
+int prepare_sliced(ct_scn* s) {
+  DeviceScenario& d = s->d;
+  cudaStream_t st = s->ctx->stream;
+  if (!d.H_sl) {
+    const int64_t sp = ct::slice_pitch(d.S), kpm = ct::slice_pitch(d.M);
+    const int64_t ngs = ct::slice_groups(d.S), ngm = ct::slice_groups(d.M);
+    int rc = alloc(s, &d.H_sl, d.B * 3 * d.M * sp);
+    if (!rc) rc = alloc(s, &d.H_sc, d.B * ngs * d.M);
+    if (!rc) rc = alloc(s, &d.Ht_sl, d.B * 3 * d.S * kpm);
+    if (!rc) rc = alloc(s, &d.Ht_sc, d.B * ngm * d.S);
+    if (!rc) rc = alloc(s, &d.X_sl, 3 * d.T * sp);
+    if (!rc) rc = alloc(s, &d.X_sc, d.T * ngs);
+    if (!rc) rc = alloc(s, &d.R_sl, 3 * d.T * kpm);
+    if (!rc) rc = alloc(s, &d.R_sc, d.T * ngm);
+    if (rc) {
+      for (void* p : {(void*)d.H_sl, (void*)d.H_sc, (void*)d.Ht_sl, (void*)d.Ht_sc, (void*)d.X_sl, (void*)d.X_sc,
+                      (void*)d.R_sl, (void*)d.R_sc})
+        release(s, p);
+      d.H_sl = d.Ht_sl = d.X_sl = d.R_sl = nullptr;
+      d.H_sc = d.Ht_sc = d.X_sc = d.R_sc = nullptr;
+      return rc;
+    }
+    d.slice_ready = false;
+  }
+  if (!d.slice_ready) {
+    CT_CUDA(ct::slice_prepare(d, st), "slicing the measurement matrix");
+    CT_CUDA(cudaStreamSynchronize(st), "slicing the measurement matrix");
+    s->launches += 3 * d.B;
+    d.slice_ready = true;
+  }
+  return CT_OK;
+}
+
 // Adjoint-mode buffers, allocated on first use (or when the checkpoint interval k changes); the
 // inbox ring grows with the delay bound.
 int prepare_adjoint(ct_scn* s, int k = ct::kCkptSteps) {
@@ -308,6 +370,11 @@ int run_beat(ct_scn* s, int64_t beat, int precision, int grad_mode) {
             "measurement kernel");
     CT_CUDA(run_phase(s, CT_PHASE_MAP_RESIDUALS, 1, [&] { return ct::launch_map_residuals(d, beat, st); }),
             "mapped-residual kernel");
+  } else if (precision == CT_PREC_BF16X6) {
+    CT_CUDA(run_phase(s, CT_PHASE_MEASURE, 4, [&] { return ct::launch_measure_sliced(d, beat, true, st); }),
+            "sliced tensor-core measurement kernel");
+    CT_CUDA(run_phase(s, CT_PHASE_MAP_RESIDUALS, 2, [&] { return ct::launch_map_residuals_sliced(d, beat, st); }),
+            "sliced tensor-core mapped-residual kernel");
   } else {
     CT_CUDA(run_phase(s, CT_PHASE_MEASURE, 3,
                       [&] { return ct::launch_measure_umma(d, beat, true, precision, st); }),
@@ -743,7 +810,7 @@ int ct_ctx_create(int device, void* stream, ct_ctx** out) {
   int count = 0;
   CT_CUDA(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
   if (device < 0 || device >= count) return fail(CT_ERR_INVALID_ARGUMENT, "device %d of %d", device, count);
-  CT_CUDA(cudaSetDevice(device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(device);
   ct_ctx* c = new ct_ctx;
   c->device = device;
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -764,7 +831,7 @@ int ct_ctx_create(int device, void* stream, ct_ctx** out) {
 namespace {
 void ctx_release(ct_ctx* ctx) {
   if (--ctx->refs > 0) return;
-  cudaSetDevice(ctx->device);
+  DeviceScope device_scope__(ctx->device);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -799,7 +866,7 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   std::vector<int32_t> nbr;
   rc = validate_and_build_nbr(desc, nbr);
   if (rc) return rc;
-  CT_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(ctx->device);
 
   ct_scn* s = new ct_scn;
   s->ctx = ctx;
@@ -832,10 +899,14 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   d.spad = (S + 3) / 4 * 4;
   d.kpad = ((M + 31) / 32) * 32;
   d.ksplit_umma = d.umma ? ct::umma_ksplit(T, S, M, ctx->num_sms) : 1;
+  d.ksplit_slice = d.umma ? ct::slice_ksplit(T, S, M, ctx->num_sms) : 1;
   const int64_t V = d.V, mpad = ((M + 63) / 64) * 64;
   const int64_t ldp_umma = ((M + ct::umma_yn(M) - 1) / ct::umma_yn(M)) * ct::umma_yn(M);
-  const int64_t part_floats = std::max<int64_t>((int64_t)d.ksplit * T * mpad,
-                                                d.umma ? (int64_t)d.ksplit_umma * T * ldp_umma : 0);
+  const int64_t ldp_slice = ((M + 127) / 128) * 128;
+  const int64_t part_floats =
+      std::max<int64_t>(std::max<int64_t>((int64_t)d.ksplit * T * mpad,
+                                          d.umma ? (int64_t)d.ksplit_umma * T * ldp_umma : 0),
+                        d.umma ? (int64_t)d.ksplit_slice * T * ldp_slice : 0);
 #define ALLOC(ptr, n)                    \
   do {                                   \
     int r__ = alloc(s, &(ptr), (n));     \
@@ -990,7 +1061,7 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
 int ct_scenario_destroy(ct_scn* scn) {
   if (!scn) return CT_OK;
   ct_ctx* ctx = scn->ctx;
-  cudaSetDevice(ctx->device);
+  DeviceScope device_scope__(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   free_scenario(scn);
   delete scn;
@@ -1034,12 +1105,15 @@ static int run_epoch_impl(ct_scn* scn, int64_t* batch_index, const int32_t* beat
   if (!scn || !batch_index) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
   if (grad_mode != CT_GRAD_REFERENCE && grad_mode != CT_GRAD_ADJOINT)
     return fail(CT_ERR_NOT_SUPPORTED, "gradient mode %d", grad_mode);
-  if (precision != CT_PREC_FP32 && precision != CT_PREC_TF32X3 && precision != CT_PREC_TF32)
-    return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
+  if (!valid_precision(precision)) return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
   if (precision != CT_PREC_FP32 && !scn->d.umma)
     return fail(CT_ERR_NOT_SUPPORTED,
                 "tensor-core precision needs the driver's TMA encoder and at most 65,536 sensor rows");
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
+  if (precision == CT_PREC_BF16X6 && !plain) {
+    int rc0 = prepare_sliced(scn);
+    if (rc0) return rc0;
+  }
   DeviceScenario& d = scn->d;
   const ct_algorithm& a = scn->algo;
   std::vector<int32_t> order((size_t)d.B);
@@ -1089,7 +1163,7 @@ int ct_run_epoch_plain(ct_scn* scn, int64_t* batch_index, const int32_t* beat_or
 
 int ct_simulate(ct_scn* scn, float* measurements_out, float* states_out) {
   if (!scn || !measurements_out) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
   DeviceScenario& d = scn->d;
   cudaStream_t st = scn->ctx->stream;
   for (int64_t beat = 0; beat < d.B; ++beat) {
@@ -1142,7 +1216,7 @@ int ct_read_field(ct_scn* scn, int field, void* dst, size_t nbytes) {
   int rc = field_bytes(scn, field, &want);
   if (rc) return rc;
   if (want != nbytes) return fail(CT_ERR_INVALID_ARGUMENT, "field %d has %zu bytes, got %zu", field, want, nbytes);
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
   DeviceScenario& d = scn->d;
   float* out = static_cast<float*>(dst);
   switch (field) {
@@ -1236,7 +1310,7 @@ int ct_write_field(ct_scn* scn, int field, const void* src, size_t nbytes) {
   int rc = field_bytes(scn, field, &want);
   if (rc) return rc;
   if (want != nbytes) return fail(CT_ERR_INVALID_ARGUMENT, "field %d has %zu bytes, got %zu", field, want, nbytes);
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
   DeviceScenario& d = scn->d;
   void* dst = nullptr;
   switch (field) {
@@ -1283,7 +1357,7 @@ int ct_write_field(ct_scn* scn, int field, const void* src, size_t nbytes) {
 
 int ct_sync(ct_scn* scn) {
   if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
   CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "cudaStreamSynchronize");
   int32_t status = 0;
   CT_CUDA(cudaMemcpy(&status, scn->d.status, sizeof(int32_t), cudaMemcpyDeviceToHost), "read status");
@@ -1302,7 +1376,7 @@ int ct_kernel_launches(ct_scn* scn, int64_t* launches) {
 
 int ct_set_profiling(ct_scn* scn, int enable) {
   if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
   CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "cudaStreamSynchronize");
   for (auto& pe : scn->pending) {
     scn->event_pool.push_back(pe.start);
@@ -1321,7 +1395,7 @@ int ct_set_profiling(ct_scn* scn, int enable) {
 
 int ct_read_profile(ct_scn* scn, double* ms, int64_t* launches) {
   if (!scn || !ms || !launches) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
   CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "cudaStreamSynchronize");
   for (auto& pe : scn->pending) {
     float t = 0.0f;
@@ -1530,6 +1604,9 @@ cudaError_t batch_enqueue_epoch(ct_batch* b) {
       if (b->precision == CT_PREC_FP32 || !d.umma) {
         B_CUDA(ct::launch_measure(d, beat, true, ss));
         B_CUDA(ct::launch_map_residuals(d, beat, ss));
+      } else if (b->precision == CT_PREC_BF16X6) {
+        B_CUDA(ct::launch_measure_sliced(d, beat, true, ss));
+        B_CUDA(ct::launch_map_residuals_sliced(d, beat, ss));
       } else {
         B_CUDA(ct::launch_measure_umma(d, beat, true, b->precision, ss));
         B_CUDA(ct::launch_map_residuals_umma(d, beat, b->precision, ss));
@@ -1745,8 +1822,7 @@ int ct_batch_create(ct_ctx* ctx, ct_scn* const* scenarios, int64_t count, int gr
   *out = nullptr;
   if (grad_mode != CT_GRAD_REFERENCE && grad_mode != CT_GRAD_ADJOINT)
     return fail(CT_ERR_NOT_SUPPORTED, "gradient mode %d", grad_mode);
-  if (precision != CT_PREC_FP32 && precision != CT_PREC_TF32X3 && precision != CT_PREC_TF32)
-    return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
+  if (!valid_precision(precision)) return fail(CT_ERR_NOT_SUPPORTED, "precision %d", precision);
   for (int64_t i = 0; i < count; ++i) {
     ct_scn* s = scenarios[i];
     if (!s) return fail(CT_ERR_INVALID_ARGUMENT, "scenario %lld is NULL", (long long)i);
@@ -1757,7 +1833,13 @@ int ct_batch_create(ct_ctx* ctx, ct_scn* const* scenarios, int64_t count, int gr
     for (int64_t j = 0; j < i; ++j)
       if (scenarios[j] == s) return fail(CT_ERR_INVALID_ARGUMENT, "scenario %lld appears twice", (long long)i);
   }
-  CT_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(ctx->device);
+  if (precision == CT_PREC_BF16X6)  // slice every member's H before the epoch graph is captured
+    for (int64_t i = 0; i < count; ++i)
+      if (scenarios[i]->d.umma) {
+        int rc0 = prepare_sliced(scenarios[i]);
+        if (rc0) return rc0;
+      }
   ct_batch* b = new ct_batch;
   b->ctx = ctx;
   b->grad_mode = grad_mode;
@@ -1824,7 +1906,7 @@ int ct_batch_create(ct_ctx* ctx, ct_scn* const* scenarios, int64_t count, int gr
 int ct_batch_destroy(ct_batch* b) {
   if (!b) return CT_OK;
   ct_ctx* ctx = b->ctx;
-  cudaSetDevice(ctx->device);
+  DeviceScope device_scope__(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   batch_free(b);
   delete b;
@@ -1834,7 +1916,7 @@ int ct_batch_destroy(ct_batch* b) {
 
 int ct_batch_run_epoch(ct_batch* b, int64_t* batch_indices) {
   if (!b || !batch_indices) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
-  CT_CUDA(cudaSetDevice(b->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(b->ctx->device);
   const size_t n = b->scns.size();
   for (size_t i = 0; i < n; ++i) {
     ct_scn* s = b->scns[i];
@@ -1873,7 +1955,7 @@ int ct_batch_run_epoch(ct_batch* b, int64_t* batch_indices) {
 
 int ct_batch_autotune(ct_batch* b, int64_t* batch_indices, int* ckpt_k, int* tile_order, double* best_ms) {
   if (!b || !batch_indices) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
-  CT_CUDA(cudaSetDevice(b->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(b->ctx->device);
   cudaStream_t st = b->ctx->stream;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CT_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
@@ -1958,7 +2040,7 @@ int ct_batch_set_profiling(ct_batch* b, int enable) {
 
 int ct_batch_read_profile(ct_batch* b, double* ms) {
   if (!b || !ms) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
-  CT_CUDA(cudaSetDevice(b->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(b->ctx->device);
   CT_CUDA(cudaStreamSynchronize(b->ctx->stream), "cudaStreamSynchronize");
   for (auto& pe : b->pending) {
     float t = 0.0f;
@@ -2111,7 +2193,7 @@ int ct_run_model_based(ct_scn* scn, const ct_run_config* cfg, const int32_t* bea
   if (!scn || !cfg || !batch_index || !summary) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
   int rc = check_run_config(cfg);
   if (rc) return rc;
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
   *summary = ct_run_summary{};
   const int64_t nsnap = cfg->snapshots_interval == 0 ? 0 : cfg->epochs / cfg->snapshots_interval + 1;
   rc = ensure_snapshots(scn, nsnap);
@@ -2154,7 +2236,7 @@ int ct_batch_run_model_based(ct_batch* batch, const ct_run_config* cfg, int64_t*
   if (cfg->snapshots_interval != 0) return fail(CT_ERR_NOT_SUPPORTED, "batched runs store no snapshots");
   if (cfg->grad_mode != batch->grad_mode || cfg->precision != batch->precision)
     return fail(CT_ERR_INVALID_ARGUMENT, "the batch was created with another gradient mode or precision");
-  CT_CUDA(cudaSetDevice(batch->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(batch->ctx->device);
   const size_t n = batch->scns.size();
   std::vector<float> original(n), lr(n), host(3 * n, 0.0f);
   for (size_t i = 0; i < n; ++i) {
@@ -2219,7 +2301,7 @@ int ct_batch_run_model_based(ct_batch* batch, const ct_run_config* cfg, int64_t*
 
 int ct_calculate_plotting_arrays(ct_scn* scn, float sample_rate_hz) {
   if (!scn) return fail(CT_ERR_INVALID_ARGUMENT, "scenario is NULL");
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
   int rc = ensure_post(scn, true);
   if (rc) return rc;
   CT_CUDA(ct::launch_spherical(scn->d, scn->post, scn->post_plan, true, sample_rate_hz, scn->ctx->stream),
@@ -2242,7 +2324,7 @@ int ct_calculate_final(ct_scn* scn, const int32_t* ground_truth_types, const int
       return fail(CT_ERR_INVALID_ARGUMENT, "voxel number %d of cell %lld is not a state index of this scenario",
                   num, (long long)g);
   }
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
   int rc = ensure_post(scn, false);
   if (rc) return rc;
   if (!scn->final_hist) {
@@ -2383,7 +2465,7 @@ int ct_measurement_matrix(ct_ctx* ctx, const ct_spatial_desc* desc, float* out, 
     for (int k = 0; k < 3; ++k) vpos[(size_t)(3 * v + k)] = desc->voxel_positions_mm[3 * cell_of[(size_t)v] + k];
     col[(size_t)v] = (int32_t)(3 * v);
   }
-  CT_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(ctx->device);
   TempBuffers tb;
   float* dH = nullptr;
   CT_CUDA(tb.get(&dH, B * M * S), "cudaMalloc");
@@ -2414,7 +2496,7 @@ int ct_scenario_set_measurement_matrix(ct_scn* scn, const ct_spatial_desc* desc)
     for (int k = 0; k < 3; ++k) vpos[(size_t)(3 * u + k)] = desc->voxel_positions_mm[3 * c + k];
     col[(size_t)u] = (int32_t)(3 * u);
   }
-  CT_CUDA(cudaSetDevice(scn->ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(scn->ctx->device);
   CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "scenario stream");
   rc = fill_lead_field(scn->ctx, desc, vpos, col, d.H, d.S);
   if (rc) return rc;
@@ -2422,6 +2504,11 @@ int ct_scenario_set_measurement_matrix(ct_scn* scn, const ct_spatial_desc* desc)
   if (d.umma) {
     CT_CUDA(ct::umma_prepare(d, scn->ctx->stream), "tensor-core operand split");
     scn->launches += 2;
+  }
+  d.slice_ready = false;
+  if (d.H_sl) {
+    rc = prepare_sliced(scn);
+    if (rc) return rc;
   }
   CT_CUDA(cudaStreamSynchronize(scn->ctx->stream), "measurement matrix");
   return CT_OK;
@@ -2438,7 +2525,7 @@ int ct_delay_samples(ct_ctx* ctx, const ct_spatial_desc* desc, float* initial_de
   if (count != V * kOffsets)
     return fail(CT_ERR_INVALID_ARGUMENT, "delay arrays have %lld elements, got %lld", (long long)(V * kOffsets),
                 (long long)count);
-  CT_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CT_DEVICE_SCOPE(ctx->device);
   cudaStream_t st = ctx->stream;
   TempBuffers tb;
   int32_t *dt = nullptr, *dn = nullptr, *dd = nullptr;

@@ -1,6 +1,7 @@
 // Internal declarations shared by the library's translation units.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -69,6 +70,17 @@ struct DeviceScenario {
   float* Xpad;           // [T,spad] copy of X for the H x operand when S % 4 != 0 (else null)
   float* Ht_hi, *Ht_lo;  // [B,S,kpad] TF32 split of H^T, zero padded
   float* R_hi, *R_lo;    // [T,kpad] TF32 split of the residuals
+  // sliced BF16 form (ct_slice.cu), allocated on first use; sp = S and kpm = M rounded up to 64
+  int ksplit_slice;          // split-K factor of the sliced H x (whole 512-element groups per split)
+  bool slice_ready;          // H_sl / Ht_sl hold the slices of the current H
+  __nv_bfloat16* H_sl;       // [B][3][M][sp] slices of H
+  float* H_sc;               // [B][ceil(sp/512)][M] scales (group-major)
+  __nv_bfloat16* Ht_sl;      // [B][3][S][kpm] slices of H^T
+  float* Ht_sc;              // [B][ceil(kpm/512)][S]
+  __nv_bfloat16* X_sl;       // [3][T][sp] slices of the beat's states
+  float* X_sc;               // [T][ceil(sp/512)]
+  __nv_bfloat16* R_sl;       // [3][T][kpm] slices of the beat's residuals
+  float* R_sc;               // [T][ceil(kpm/512)]
   int32_t* dmin;         // [2] smallest and largest delay of a connected (voxel, offset) pair
   // resident forward form (one tile per CTA, halo history in a shared ring)
   bool fwd_ring;
@@ -156,6 +168,15 @@ cudaError_t umma_prepare(DeviceScenario& d, cudaStream_t stream);
 cudaError_t launch_measure_umma(DeviceScenario& d, int64_t beat, bool with_residuals, int precision,
                                 cudaStream_t stream);
 cudaError_t launch_map_residuals_umma(DeviceScenario& d, int64_t beat, int precision, cudaStream_t stream);
+// Sliced BF16 forms (ct_slice.cu): K extents rounded up to whole 64-element chunks, scale groups of
+// 512 elements, the split-K factor of H x, the slicing of H and H^T (after every change of H;
+// allocates and frees a temporary [S, kpm] buffer on the stream), and the two products.
+int64_t slice_pitch(int64_t k);
+int64_t slice_groups(int64_t k);
+int slice_ksplit(int64_t T, int64_t S, int64_t M, int sms);
+cudaError_t slice_prepare(DeviceScenario& d, cudaStream_t stream);
+cudaError_t launch_measure_sliced(DeviceScenario& d, int64_t beat, bool with_residuals, cudaStream_t stream);
+cudaError_t launch_map_residuals_sliced(DeviceScenario& d, int64_t beat, cudaStream_t stream);
 
 struct DeriveScalars {
   float mse_scaling, reg_scaling, threshold, diffreg;

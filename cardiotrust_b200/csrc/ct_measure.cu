@@ -212,6 +212,20 @@ extern "C" int ct_predict_measurements_noalloc(const float* states, const float*
   cudaError_t err = cudaGetDevice(&device);
   if (err != cudaSuccess || device < 0 || device >= kMaxDevices)
     return report_error(CT_ERR_CUDA, "cudaGetDevice failed or device index out of range");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (st) {
+    // the scratch address below is the current device's; a stream of another device would make the
+    // kernels write into memory that device does not own
+    int stream_device = -1;
+    err = cudaStreamGetDevice(st, &stream_device);
+    if (err != cudaSuccess) return report_error(CT_ERR_INVALID_ARGUMENT, "cudaStreamGetDevice failed on the stream");
+    if (stream_device != device) {
+      char msg[160];
+      std::snprintf(msg, sizeof(msg), "the stream belongs to device %d but device %d is current", stream_device,
+                    device);
+      return report_error(CT_ERR_INVALID_ARGUMENT, msg);
+    }
+  }
   float* scratch = nullptr;
   int rc = scratch_address(device, &scratch);
   if (rc) return rc;
@@ -228,7 +242,6 @@ extern "C" int ct_predict_measurements_noalloc(const float* states, const float*
   if (ks > by_scratch) ks = by_scratch;
   if (ks < 1) ks = 1;
   const int64_t kchunk = ((S + ks - 1) / ks + BK - 1) / BK * BK;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   // every (split, step, sensor) partial read below is written first, so nothing is cleared
   dim3 grid((unsigned)((M + BN - 1) / BN), (unsigned)((T + BM - 1) / BM), (unsigned)ks);
   gemm_kernel<true><<<grid, kThreads, 0, st>>>(states, S, measurement_matrix, S, scratch, mpad, T * mpad, T, M, S,

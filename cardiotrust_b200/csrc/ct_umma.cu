@@ -31,128 +31,24 @@
 #include <mutex>
 
 #include "ct_internal.cuh"
+#include "ct_tcgen05.cuh"
 
 namespace ct {
 namespace {
 
+using namespace tc;
+
 constexpr int kBM = 128;          // output rows per tile (tensor-memory lanes)
 // K chunks accumulated in tensor memory before the epilogue adds them into the promoted FP32 sum.
-// The tensor core's accumulation over long chains drifts (its adds are not round-to-nearest);
-// promoting every few chunks keeps the product at FP32 quality (measured on the 768-row
-// precision config: relative error of H x 6e-6 without promotion, FP32-level with it).
+// The tensor core's accumulation over long chains drifts toward zero (its adds are not
+// round-to-nearest). Promoting every 8 chunks cuts the relative error of H x 3x (6e-6 to 1.8e-6
+// on 768 sensor rows x 141,792 states) but does not remove its bias: gradients of configs whose
+// residuals are a small fraction of the signal stay ~20x above the FP32 CUDA-core products'
+// error. The sliced BF16 products (ct_slice.cu) accumulate exactly and do not have this bias.
 constexpr int kPromote = 8;
 constexpr int kBK = 32;           // K elements per chunk (one 128-byte swizzle row of f32)
 constexpr int kUmmaK = 8;         // K per tf32 MMA instruction
 constexpr int kThreadsUmma = 192;  // 6 warps
-constexpr unsigned long long kWaitNs = 2000000000ull;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait for the completion of the phase with the given parity.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t* status, volatile int* abort_flag) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = globaltimer();
-  while (true) {
-    if (mbar_try(bar, parity)) return true;
-    if (*abort_flag) return false;
-    if (globaltimer() - t0 > kWaitNs) {
-      atomicCAS(status, 0, (int32_t)CT_ERR_TIMEOUT);
-      *abort_flag = 1;
-      return false;
-    }
-  }
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
-          "r"(smem_u32(dst)),
-      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
-      : "memory");
-}
-
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);  // start address, bits [0,14)
-  d |= (uint64_t)1 << 16;                   // leading byte offset (unused for swizzled K-major) = 16 B
-  d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset = 1024 B
-  d |= (uint64_t)1 << 46;                   // descriptor version for sm_100
-  d |= (uint64_t)2 << 61;                   // layout: 128-byte swizzle
-  return d;
-}
-
-// Instruction descriptor: kind::tf32, FP32 accumulate, both operands K-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t tf32_idesc(int n) {
-  return (1u << 4)                    // D format F32
-         | (2u << 7)                  // A format TF32
-         | (2u << 10)                 // B format TF32
-         | ((uint32_t)(n >> 3) << 17)  // N >> 3
-         | ((uint32_t)(kBM >> 4) << 24);  // M >> 4
-}
-
-__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
-      "[%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16};" ::"r"(taddr),
-      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
-      "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
-      "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
-      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
-      : "memory");
-}
 
 __device__ __forceinline__ float tf32_rna(float x) {
   uint32_t r;
@@ -458,12 +354,9 @@ __global__ void reduce_split_kernel(const float* __restrict__ part, int ksplit, 
   }
 }
 
-// ---- host: tensor maps
+}  // namespace
 
-using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
+namespace tc {
 EncodeTiledFn encode_fn() {
   static std::once_flag once;
   static EncodeTiledFn fn = nullptr;
@@ -476,6 +369,9 @@ EncodeTiledFn encode_fn() {
   });
   return fn;
 }
+}  // namespace tc
+
+namespace {
 
 // 2D row-major f32 matrix [rows][inner] (inner contiguous), box = 32 x box_rows, 128-byte swizzle.
 bool make_map(CUtensorMap* map, const float* ptr, int64_t inner, int64_t rows, int box_rows) {

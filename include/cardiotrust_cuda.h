@@ -73,8 +73,14 @@ enum ct_grad_mode {
 /* Arithmetic of the two measurement products (H x and H^T r). */
 enum ct_precision {
   CT_PREC_FP32 = 0,   /* FP32 CUDA-core GEMMs */
-  CT_PREC_TF32X3 = 1, /* tcgen05 TF32 with a hi/lo split of both operands (hi*hi + hi*lo + lo*hi), FP32 accumulate */
-  CT_PREC_TF32 = 2    /* tcgen05 TF32, one pass (operands rounded to TF32) */
+  CT_PREC_TF32X3 = 1, /* tcgen05 TF32 with a hi/lo split of both operands (hi*hi + hi*lo + lo*hi), FP32
+                         accumulate. The tensor core's accumulation is biased toward zero: when residuals are a
+                         small fraction of the signal, gradients drift ~1e-2 from the FP64 result. */
+  CT_PREC_TF32 = 2,   /* tcgen05 TF32, one pass (operands rounded to TF32) */
+  CT_PREC_BF16X6 = 3  /* tcgen05 BF16 on error-free slices: every operand row is cut into groups of 512 values
+                         sharing a power-of-two scale and split into three 8-bit integer slices (exact in BF16);
+                         six slice products accumulate exactly in FP32 tensor memory and are folded into an FP32
+                         sum, rounding to nearest, every 512 values. Unbiased like FP32 CUDA-core products. */
 };
 
 /* The Algorithm fields the epoch reads, src/core/config/algorithm.rs:25-58. */
@@ -418,12 +424,14 @@ int ct_output_state_indices(const ct_spatial_desc* desc, int32_t* out, size_t nb
  *
  * predicted[t, m] = sum_s measurement_matrix[m, s] * states[t, s] for one beat, and, when
  * residuals is non-NULL, residuals = predicted - actual (all [T, M]). All pointers are device
- * pointers owned by the caller; work is enqueued on `stream` (NULL = legacy default stream).
+ * pointers owned by the caller; work is enqueued on `stream` (NULL = legacy default stream), which
+ * must belong to the current device (CT_ERR_INVALID_ARGUMENT otherwise).
  * Split-K partial sums go to one 8 MiB file-scope device array that every GPU loading the
  * library holds until exit; num_steps x ceil(num_sensors / 64) x 64 must not exceed 2,097,152
  * (CT_ERR_INVALID_ARGUMENT otherwise). The first call on a device looks up that array's device
- * address (cudaGetSymbolAddress) with the device current; make that first call before any
- * stream capture. The function calls no cudaMalloc / cudaFree. All calls share the array:
+ * address (cudaGetSymbolAddress) with the device current and keeps it; make that first call before any
+ * stream capture. A device reset (cudaDeviceReset) invalidates the kept address: do not call this
+ * function after resetting a device it has run on. The function calls no cudaMalloc / cudaFree. All calls share the array:
  * calls that overlap on the GPU (other streams, other host threads) race on it. */
 int ct_predict_measurements_noalloc(const float* states, const float* measurement_matrix, const float* actual,
                                     float* predicted, float* residuals, int64_t num_steps, int64_t num_states,

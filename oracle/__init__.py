@@ -23,7 +23,7 @@ _BUILD = _HERE / "_build"
 _LIB_PATH = _BUILD / "liboracle.so"
 _lib = None
 
-CXXFLAGS = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math", "-std=c++17", "-shared", "-fPIC"]
+CXXFLAGS = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math", "-std=c++17", "-shared", "-fPIC", "-fopenmp"]
 
 
 def build(force: bool = False) -> pathlib.Path:
@@ -46,7 +46,19 @@ def lib():
         _lib.oracle_from_samples_to_coef.argtypes = [ctypes.c_float]
         _lib.oracle_from_coef_to_samples.restype = ctypes.c_float
         _lib.oracle_from_coef_to_samples.argtypes = [ctypes.c_float]
+        _lib.oracle_set_threads.argtypes = [ctypes.c_int]
+        _lib.oracle_max_threads.restype = ctypes.c_int
     return _lib
+
+
+def set_threads(n: int) -> None:
+    """Threads of the oracle's parallel loops, process-wide (0 = OpenMP's default, all cores). Only
+    loops over independent outputs run in parallel, so every result is bit-identical for any count."""
+    lib().oracle_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().oracle_max_threads())
 
 
 class Algo(ctypes.Structure):

@@ -25,6 +25,8 @@
 // summation order is not pinned by any test in the reference tree, so the
 // GPU is compared against these products with a tolerance, never bitwise.
 
+#include <omp.h>
+
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -98,6 +100,15 @@ struct Epoch {
   // optional: receives H^T r per (beat, step) [B,T,S]
   T* mapped_residuals_history;
 };
+
+// ---------------------------------------------------------------- threads
+
+// Thread count of the parallel loops (0 = OpenMP's default). Only loops whose iterations write
+// disjoint outputs, each in the reference's own order, run in parallel, so every result is
+// bit-identical for any count. Process-wide, so replicas run from several host threads can ask for
+// one thread each.
+int g_threads = 0;
+inline int oracle_threads() { return g_threads > 0 ? g_threads : omp_get_max_threads(); }
 
 // ---------------------------------------------------------------- ndarray / matrixmultiply
 
@@ -186,6 +197,8 @@ void innovate_system_states(Epoch<T>& e, int64_t step) {
   const int64_t S = e.num_states;
   std::memcpy(e.ap_outputs_last, e.ap_outputs_now, sizeof(T) * S * kGainCols);
   T* x_now = e.system_states + step * S;
+  // every state's sum is computed by one thread in the reference's k order
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
   for (int64_t i = 0; i < S; ++i) {
     for (int k = 0; k < kGainCols; ++k) {
       const int32_t out = e.output_state_indices[i * kGainCols + k];
@@ -218,6 +231,7 @@ void predict_measurements(Epoch<T>& e, int64_t beat, int64_t step) {
   const T* H = e.measurement_matrix + beat * M * S;
   const T* x = e.system_states + step * S;
   T* y = e.measurements + (beat * Tn + step) * M;
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
   for (int64_t m = 0; m < M; ++m) y[m] = unrolled_dot(H + m * S, x, S) * T(1);
 }
 
@@ -241,15 +255,24 @@ void calculate_mapped_residuals(Epoch<T>& e, int64_t beat, int64_t step) {
   } else {
     const T* H = e.measurement_matrix + beat * M * S;
     constexpr int64_t KC = 256;
-    for (int64_t s = 0; s < S; ++s) {
-      T c = 0;
+    // per state s: c = sum over KC-blocks (in order) of the block's fma chain in m order. The loops
+    // run m-outer over a block of states (rows of H streamed), which keeps every state's order.
+    constexpr int64_t SB = 512;
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
+    for (int64_t s0 = 0; s0 < S; s0 += SB) {
+      const int64_t s1 = (s0 + SB < S) ? s0 + SB : S;
+      T c[SB], ab[SB];
       for (int64_t k0 = 0; k0 < M; k0 += KC) {
         const int64_t k1 = (k0 + KC < M) ? k0 + KC : M;
-        T ab = 0;
-        for (int64_t m = k0; m < k1; ++m) ab = std::fma(H[m * S + s], e.residuals[m], ab);
-        c = (k0 == 0) ? ab : ab + c;
+        for (int64_t s = s0; s < s1; ++s) ab[s - s0] = 0;
+        for (int64_t m = k0; m < k1; ++m) {
+          const T rm = e.residuals[m];
+          const T* Hm = H + m * S;
+          for (int64_t s = s0; s < s1; ++s) ab[s - s0] = std::fma(Hm[s], rm, ab[s - s0]);
+        }
+        for (int64_t s = s0; s < s1; ++s) c[s - s0] = (k0 == 0) ? ab[s - s0] : ab[s - s0] + c[s - s0];
       }
-      e.mapped_residuals[s] = c;
+      for (int64_t s = s0; s < s1; ++s) e.mapped_residuals[s] = M > 0 ? c[s - s0] : T(0);
     }
   }
   if (e.mapped_residuals_history)
@@ -262,20 +285,28 @@ void calculate_maximum_regularization(Epoch<T>& e, int64_t step, T threshold) {
   const int64_t S = e.num_states;
   const T* x = e.system_states + step * S;
   T* mr = e.maximum_regularization;
+  // the per-voxel terms in parallel, their running sum in voxel order
+  std::vector<T> sq((size_t)(S / 3));
+  std::vector<char> over((size_t)(S / 3));
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
   for (int64_t i = 0; i < S; i += 3) {
     const T sum = std::fabs(x[i]) + std::fabs(x[i + 1]) + std::fabs(x[i + 2]);
     if (sum > threshold) {
       const T factor = sum - threshold;
-      *e.maximum_regularization_sum += factor * factor;
+      sq[(size_t)(i / 3)] = factor * factor;
+      over[(size_t)(i / 3)] = 1;
       mr[i] = factor * signum(x[i]);
       mr[i + 1] = factor * signum(x[i + 1]);
       mr[i + 2] = factor * signum(x[i + 2]);
     } else {
+      over[(size_t)(i / 3)] = 0;
       mr[i] = 0;
       mr[i + 1] = 0;
       mr[i + 2] = 0;
     }
   }
+  for (int64_t v = 0; v < S / 3; ++v)
+    if (over[(size_t)v]) *e.maximum_regularization_sum += sq[(size_t)v];
 }
 
 // calculate_derivatives_gains, derivation.rs:307-329
@@ -284,6 +315,7 @@ void calculate_derivatives_gains(Epoch<T>& e, const Algo& a) {
   const int64_t S = e.num_states;
   const T mse_scaling = T(1) / static_cast<T>(e.num_sensors) * static_cast<T>(a.mse_strength);
   const T reg_scaling = static_cast<T>(a.maximum_regularization_strength);
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
   for (int64_t i = 0; i < S; ++i) {
     const T max_reg = e.maximum_regularization[i];
     const T residual = e.mapped_residuals[i];
@@ -306,7 +338,10 @@ void calculate_derivatives_coefs_simple(Epoch<T>& e, int64_t step, const Algo& a
   const int64_t S = e.num_states;
   const T mse_scaling = T(1) / static_cast<T>(e.num_sensors) * static_cast<T>(a.mse_strength);
   const T diff = static_cast<T>(a.difference_regularization_strength);
-  for (int64_t i = 0; i < S; ++i) {
+  // parallel over voxels: d_coefs[ci] of voxel v receives its terms from rows 3v..3v+2 only, in order
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
+  for (int64_t v = 0; v < S / 3; ++v)
+  for (int64_t i = 3 * v; i < 3 * v + 3; ++i) {
     for (int k = 0; k < kGainCols; ++k) {
       const int64_t ci = (i / 3) * kOffsets + k / 3;
       const T dd = delay_delta(e, ci);
@@ -330,6 +365,7 @@ void calculate_derivatives_coefs_textbook(Epoch<T>& e, int64_t step, const Algo&
   const int64_t S = e.num_states;
   const T mse_scaling = T(1) / static_cast<T>(e.num_sensors) * static_cast<T>(a.mse_strength);
   const T diff = static_cast<T>(a.difference_regularization_strength);
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
   for (int64_t i = 0; i < S; ++i) {
     for (int k = 0; k < kGainCols; ++k) {
       const int32_t out = e.output_state_indices[i * kGainCols + k];
@@ -343,6 +379,7 @@ void calculate_derivatives_coefs_textbook(Epoch<T>& e, int64_t step, const Algo&
       }
     }
   }
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
   for (int64_t i = 0; i < S; ++i) {
     for (int k = 0; k < kGainCols; ++k) {
       const int64_t ci = (i / 3) * kOffsets + k / 3;
@@ -353,7 +390,9 @@ void calculate_derivatives_coefs_textbook(Epoch<T>& e, int64_t step, const Algo&
       }
     }
   }
-  for (int64_t i = 0; i < S; ++i) {
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
+  for (int64_t v = 0; v < S / 3; ++v)
+  for (int64_t i = 3 * v; i < 3 * v + 3; ++i) {
     for (int k = 0; k < kGainCols; ++k) {
       const int64_t ci = (i / 3) * kOffsets + k / 3;
       const T dd = delay_delta(e, ci);
@@ -648,21 +687,32 @@ void simulate(Epoch<T>& e) {
 // t >= d, derivation.rs:366-390), i.e. count * diff * delta^5.
 //
 // The all-pass outputs of (v, n, b) do not depend on the gain row's output
-// component a, so they are kept per voxel: aph[t][v][k], k = 3n + b.
+// component a, so they are kept per voxel: ap[t][v][k], k = 3n + b. The forward
+// stores the all-pass state every kAdjCkpt steps; the backward recomputes each
+// segment's outputs from its checkpoint and the stored states with the forward's
+// own expression (bit-identical values), so memory is O(T/K + K) planes, not O(T).
+constexpr int64_t kAdjCkpt = 64;
+
 template <typename T>
 T adjoint_beat(Epoch<T>& e, const Algo& a, int64_t beat, bool want_grad) {
   const int64_t S = e.num_states, V = e.num_voxels, M = e.num_sensors, Tn = e.num_steps;
   const T mse_scaling = T(1) / static_cast<T>(M) * static_cast<T>(a.mse_strength);
   const T reg = static_cast<T>(a.maximum_regularization_strength);
   const T thr = static_cast<T>(a.maximum_regularization_threshold);
-  std::vector<T> aph((size_t)Tn * V * kGainCols);
+  const int64_t plane = V * kGainCols;
+  const int64_t nck = (Tn + kAdjCkpt - 1) / kAdjCkpt;
+  std::vector<T> ck(want_grad ? (size_t)(nck * plane) : 0);  // ck[s] = all-pass state entering step s K
   estimations_reset(e);
   T loss = 0;
   for (int64_t t = 0; t < Tn; ++t) {
+    if (want_grad && t % kAdjCkpt == 0) {
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
+      for (int64_t v = 0; v < V; ++v)
+        std::memcpy(&ck[(size_t)((t / kAdjCkpt) * plane + v * kGainCols)], e.ap_outputs_now + 3 * v * kGainCols,
+                    sizeof(T) * kGainCols);
+    }
     system_prediction(e, beat, t);
     calculate_residuals(e, beat, t);
-    for (int64_t v = 0; v < V; ++v)
-      std::memcpy(&aph[((size_t)t * V + v) * kGainCols], e.ap_outputs_now + 3 * v * kGainCols, sizeof(T) * kGainCols);
     T rr = 0;
     for (int64_t m = 0; m < M; ++m) rr += e.residuals[m] * e.residuals[m];
     T rg = 0;
@@ -677,21 +727,61 @@ T adjoint_beat(Epoch<T>& e, const Algo& a, int64_t beat, bool want_grad) {
 
   const T* H = e.measurement_matrix + beat * M * S;
   std::vector<T> acc((size_t)Tn * S, T(0)), lam_x(S), lap((size_t)V * kGainCols, T(0)), r(M);
+  std::vector<T> seg((size_t)((kAdjCkpt + 1) * plane));  // seg[q] = all-pass output of step s K + q - 1
+  std::vector<T> lnew_all((size_t)plane);
+  int64_t seg_of = -1;
   for (int64_t t = Tn - 1; t >= 0; --t) {
+    const int64_t sg = t / kAdjCkpt;
+    if (sg != seg_of) {  // recompute the segment's all-pass outputs from its checkpoint
+      const int64_t t0 = sg * kAdjCkpt, t1 = std::min<int64_t>(Tn, t0 + kAdjCkpt);
+      std::memcpy(seg.data(), &ck[(size_t)(sg * plane)], sizeof(T) * plane);
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
+      for (int64_t v = 0; v < V; ++v)
+        for (int k = 0; k < kGainCols; ++k) {
+          const int32_t out = e.output_state_indices[(3 * v) * kGainCols + k];
+          const int64_t ci = v * kOffsets + k / 3;
+          T ap = seg[(size_t)(v * kGainCols + k)];
+          for (int64_t tt = t0; tt < t1; ++tt) {
+            if (out >= 0) {  // innovate_system_states_v1's expression (prediction.rs:68-79)
+              const int64_t delay = e.delays[ci];
+              const T input = (delay <= tt) ? e.system_states[(tt - delay) * S + out] : T(0);
+              const T input_delayed = (delay < tt) ? e.system_states[(tt - delay - 1) * S + out] : T(0);
+              ap = std::fma(e.coefs[ci], input - ap, input_delayed);
+            }
+            seg[(size_t)((tt - t0 + 1) * plane + v * kGainCols + k)] = ap;
+          }
+        }
+      seg_of = sg;
+    }
+    const int64_t q = t - sg * kAdjCkpt;
+    const T* ap_now_plane = &seg[(size_t)((q + 1) * plane)];
+    const T* ap_prev_plane = &seg[(size_t)(q * plane)];
     const T* x = e.system_states + t * S;
     const T* y = e.measurements + (beat * Tn + t) * M;
     const T* z = e.actual_measurements + (beat * Tn + t) * M;
     for (int64_t m = 0; m < M; ++m) r[m] = y[m] - z[m];
-    for (int64_t v = 0; v < V; ++v) {
-      const T s = std::fabs(x[3 * v]) + std::fabs(x[3 * v + 1]) + std::fabs(x[3 * v + 2]);
-      const T f = s > thr ? s - thr : T(0);
-      for (int c = 0; c < 3; ++c) {
-        const int64_t i = 3 * v + c;
-        T mr = 0;
-        for (int64_t m = 0; m < M; ++m) mr += H[m * S + i] * r[m];
-        lam_x[i] = mse_scaling * mr + reg * f * signum(x[i]) + acc[(size_t)t * S + i];
+    // mr_i = sum over m in order of H[m,i] r[m], computed m-outer over blocks of states
+    constexpr int64_t SB = 512;
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
+    for (int64_t s0 = 0; s0 < S; s0 += SB) {
+      const int64_t s1 = (s0 + SB < S) ? s0 + SB : S;
+      T mrb[SB];
+      for (int64_t i = s0; i < s1; ++i) mrb[i - s0] = 0;
+      for (int64_t m = 0; m < M; ++m) {
+        const T rm = r[m];
+        const T* Hm = H + m * S;
+        for (int64_t i = s0; i < s1; ++i) mrb[i - s0] += Hm[i] * rm;
+      }
+      for (int64_t i = s0; i < s1; ++i) {
+        const int64_t v = i / 3;
+        const T s = std::fabs(x[3 * v]) + std::fabs(x[3 * v + 1]) + std::fabs(x[3 * v + 2]);
+        const T f = s > thr ? s - thr : T(0);
+        lam_x[i] = mse_scaling * mrb[i - s0] + reg * f * signum(x[i]) + acc[(size_t)t * S + i];
       }
     }
+    // per (v, n, b): the voxel's own gradients and adjoint state in parallel; the contributions to
+    // earlier steps' state adjoints (acc, which this step does not read) in (v, n, b) order afterwards
+#pragma omp parallel for schedule(static) num_threads(oracle_threads())
     for (int64_t v = 0; v < V; ++v) {
       for (int n = 0; n < kOffsets; ++n) {
         const int32_t out0 = e.output_state_indices[(3 * v) * kGainCols + 3 * n];
@@ -705,15 +795,29 @@ T adjoint_beat(Epoch<T>& e, const Algo& a, int64_t beat, bool want_grad) {
           T G = 0;
           for (int c3 = 0; c3 < 3; ++c3) G += e.gains[(3 * v + c3) * kGainCols + k] * lam_x[3 * v + c3];
           const T lnew = G - c * lap[v * kGainCols + k];
-          const T ap_t = aph[((size_t)t * V + v) * kGainCols + k];
-          const T ap_prev = t > 0 ? aph[((size_t)(t - 1) * V + v) * kGainCols + k] : T(0);
+          const T ap_t = ap_now_plane[v * kGainCols + k];
+          const T ap_prev = ap_prev_plane[v * kGainCols + k];
           const T in = (d <= t) ? e.system_states[(t - d) * S + j] : T(0);
           if (!a.freeze_gains)
             for (int c3 = 0; c3 < 3; ++c3) e.d_gains[(3 * v + c3) * kGainCols + k] += lam_x[3 * v + c3] * ap_t;
           if (!a.freeze_delays) e.d_coefs[ci] += lnew * (in - ap_prev);
+          lnew_all[(size_t)(v * kGainCols + k)] = lnew;
+          lap[v * kGainCols + k] = lnew;
+        }
+      }
+    }
+    for (int64_t v = 0; v < V; ++v) {
+      for (int n = 0; n < kOffsets; ++n) {
+        const int32_t out0 = e.output_state_indices[(3 * v) * kGainCols + 3 * n];
+        if (out0 < 0) continue;
+        const int64_t ci = v * kOffsets + n;
+        const T c = e.coefs[ci];
+        const int64_t d = e.delays[ci];
+        for (int b = 0; b < 3; ++b) {
+          const T lnew = lnew_all[(size_t)(v * kGainCols + 3 * n + b)];
+          const int64_t j = out0 + b;
           if (t - d >= 0) acc[(size_t)(t - d) * S + j] += c * lnew;
           if (t - d - 1 >= 0) acc[(size_t)(t - d - 1) * S + j] += lnew;
-          lap[v * kGainCols + k] = lnew;
         }
       }
     }
@@ -1109,6 +1213,9 @@ void oracle_calculate_final_f32(const float* X, int64_t T, int64_t S, const int3
 }
 
 int oracle_abi_version() { return 1; }
+// Threads of the parallel loops (every result is independent of the count).
+void oracle_set_threads(int n) { g_threads = n > 0 ? n : 0; }
+int oracle_max_threads() { return oracle_threads(); }
 
 int oracle_run_epoch_adjoint_f64(Epoch<double>* e, const Algo* a, const int32_t* beat_order, int64_t* batch_index) {
   return run_epoch_adjoint(*e, *a, beat_order, batch_index);

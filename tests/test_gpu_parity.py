@@ -287,10 +287,11 @@ def test_reference_shaped_api(alg, ctx, oracle_mod, cuboid8):
     eng.close()
 
 
-@pytest.mark.parametrize("precision,tol_meas,tol_grad", [(1, TOL_MEAS, TOL_GRAD), (2, 5e-4, 5e-3)])
+@pytest.mark.parametrize("precision,tol_meas,tol_grad", [(1, TOL_MEAS, TOL_GRAD), (2, 5e-4, 5e-3),
+                                                         (3, TOL_MEAS, TOL_GRAD)])
 def test_tensor_core_precisions(alg, ctx, oracle_mod, cuboid8, precision, tol_meas, tol_grad):
-    """tcgen05 measurement products: split TF32 keeps the FP32 bars; one-pass TF32 has looser,
-    stated bars (operands rounded to 10-bit mantissas)."""
+    """tcgen05 measurement products: split TF32 and the sliced BF16 products keep the FP32 bars;
+    one-pass TF32 has looser, stated bars (operands rounded to 10-bit mantissas)."""
     a, oa = algo_pair(alg, oracle_mod, optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
     eng = alg.EpochEngine.from_scenario(ctx, cuboid8, num_batch_slots=2, algorithm=a)
     o = oracle_mod.from_scenario(cuboid8, num_batch_slots=2)
@@ -322,7 +323,7 @@ def test_tensor_core_shapes(alg, ctx, oracle_mod):
     a, oa = algo_pair(alg, oracle_mod, learning_rate=0.5, freeze_delays=False)
     o64 = oracle_mod.from_scenario(scn, dtype=np.float64)
     o64.run_epoch(oa)
-    for precision in (alg.Precision.Fp32, alg.Precision.Tf32x3):
+    for precision in (alg.Precision.Fp32, alg.Precision.Tf32x3, alg.Precision.Bf16x6):
         eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=a)
         eng.run_epoch(0, precision=precision)
         assert rel_err(eng.read("measurements"), o64.measurements) < TOL_MEAS, precision
@@ -342,7 +343,7 @@ def test_tensor_core_many_sensor_rows(alg, ctx, oracle_mod):
     a, oa = algo_pair(alg, oracle_mod, optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
     o64 = oracle_mod.from_scenario(scn, dtype=np.float64)
     o64.run_epoch(oa)
-    for precision in (alg.Precision.Tf32x3, alg.Precision.Tf32):
+    for precision in (alg.Precision.Tf32x3, alg.Precision.Tf32, alg.Precision.Bf16x6):
         eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=a)
         eng.run_epoch(0, precision=precision)
         loose = precision == alg.Precision.Tf32
@@ -368,12 +369,13 @@ def test_tensor_core_state_count_not_multiple_of_4(alg, ctx, oracle_mod, shape):
     adj = oracle_mod.from_scenario(scn, dtype=np.float64)
     adj.run_epoch(oa, adjoint=True)
     for mode, ref in ((alg.GradMode.Reference, o64), (alg.GradMode.Adjoint, adj)):
-        eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=a)
-        eng.run_epoch(0, grad_mode=mode, precision=alg.Precision.Tf32x3)
-        assert rel_err(eng.read("measurements"), ref.measurements) < TOL_MEAS, mode
-        assert rel_err(eng.read("grad_gains"), ref.d_gains) < TOL_GRAD, mode
-        assert rel_err(eng.read("grad_coefs"), ref.d_coefs) < TOL_GRAD, mode
-        eng.close()
+        for precision in (alg.Precision.Tf32x3, alg.Precision.Bf16x6):
+            eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=a)
+            eng.run_epoch(0, grad_mode=mode, precision=precision)
+            assert rel_err(eng.read("measurements"), ref.measurements) < TOL_MEAS, (mode, precision)
+            assert rel_err(eng.read("grad_gains"), ref.d_gains) < TOL_GRAD, (mode, precision)
+            assert rel_err(eng.read("grad_coefs"), ref.d_coefs) < TOL_GRAD, (mode, precision)
+            eng.close()
 
 
 def _mr_history(o64, scn):
