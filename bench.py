@@ -46,7 +46,6 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default=WORKLOAD)
-    p.add_argument("--cpu-steps", type=int, default=200, help="steps of the bounded CPU sample")
     p.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "tf32", "bf16x6"],
                    help="measurement products: FP32 CUDA cores, tcgen05 split TF32, tcgen05 TF32")
     p.add_argument("--batch-scenarios", type=int, default=64,
@@ -135,66 +134,74 @@ class ClockSampler:
 # ----------------------------------------------------------------------------------------- CPU
 
 
-def cpu_sample(scn, cpu_steps: int, threads: int = 1):
-    """The CPU restatement (oracle/, reference loop order, f32) on the first `cpu_steps`
-    steps of the workload, `threads` independent replicas in parallel (one scenario per
-    thread, as the reference scheduler runs scenarios). Returns (scenario-epochs/s, seconds)."""
+def _cpu_epoch(scn, steps=None):
+    """One oracle epoch object (f32, reference loop order) of the workload's first `steps` steps."""
     import numpy as np
 
     import oracle
 
-    T = min(cpu_steps, scn.num_steps)
+    T = scn.num_steps if steps is None else min(steps, scn.num_steps)
+    return oracle.OracleEpoch(
+        scn.model.gains, scn.model.output_state_indices, scn.model.coefs, scn.model.delays,
+        scn.model.initial_delays, scn.measurement_matrix, scn.control_matrix, scn.control_function[:T],
+        np.ascontiguousarray(scn.measurements[:, :T]), num_batch_slots=1)
+
+
+def cpu_epoch_time(scn, threads: int, steps=None):
+    """Seconds of one epoch of the CPU restatement (oracle/, f32, reference loop order, bit-identical for
+    any thread count) with `threads` OpenMP threads over independent outputs."""
+    import oracle
+
     cfg = oracle.algo(optimizer=1, learning_rate=1e-3, freeze_delays=0)
-    epochs = []
-    for _ in range(threads):
-        epochs.append(oracle.OracleEpoch(
-            scn.model.gains, scn.model.output_state_indices, scn.model.coefs, scn.model.delays,
-            scn.model.initial_delays, scn.measurement_matrix, scn.control_matrix, scn.control_function[:T],
-            np.ascontiguousarray(scn.measurements[:, :T]), num_batch_slots=1))
-    ts = [threading.Thread(target=e.run_epoch, args=(cfg,)) for e in epochs]
+    e = _cpu_epoch(scn, steps)
+    oracle.set_threads(threads)
     t0 = time.perf_counter()
-    for t in ts:
-        t.start()
-    for t in ts:
-        t.join()
+    e.run_epoch(cfg)
     dt = time.perf_counter() - t0
-    # each replica did T/scn.num_steps of one full epoch
-    return threads * (T / scn.num_steps) / dt, dt
+    oracle.set_threads(0)
+    return dt
+
+
+def host_cores():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
 
 
 def reference_arm(args):
+    """The reference's CPU epoch on the host cores: the f32 restatement of run_epoch (oracle/; the
+    Rust crate cannot be built in this image), with every host core (OpenMP over independent outputs:
+    results bit-identical to one thread). The K steps are one full epoch of the workload: step k is its
+    time steps [k T / K, (k + 1) T / K), so the timed region is exactly one epoch and nothing is
+    extrapolated (later steps run slower than early ones: decaying states become subnormal). Warm-up:
+    W runs of the first T / K time steps. The reference's own threading (one thread: ndarray without
+    rayon) is timed on a bounded sample, the first T / 5 steps, and reported beside it."""
     rank, _, world = dist_env()
     if rank != 0:
         return 0
-    from cardiotrust_b200 import scenario as sc
+    import numpy as np
 
     import oracle
+    from cardiotrust_b200 import scenario as sc
 
     oracle.build()
     scn = sc.build(sc.workload_spec(args.workload, seed=0))
-    # ground truth on the CPU restatement: forward of the truth model on the sampled steps
-    T = min(args.cpu_steps, scn.num_steps)
-    o = oracle.OracleEpoch(scn.truth.gains, scn.truth.output_state_indices, scn.truth.coefs, scn.truth.delays,
-                           scn.truth.initial_delays, scn.measurement_matrix, scn.control_matrix,
-                           scn.control_function[:T])
-    import numpy as np
-
-    y = o.simulate()
-    full = np.zeros((scn.num_beats, scn.num_steps, scn.num_sensors), np.float32)
-    full[:, :T] = y
-    scn.measurements = full
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    t = scn.truth
+    o = oracle.OracleEpoch(t.gains, t.output_state_indices, t.coefs, t.delays, t.initial_delays,
+                           scn.measurement_matrix, scn.control_matrix, scn.control_function)
+    y = o.simulate().astype(np.float64)
+    del o
+    rng = np.random.default_rng(scn.spec.seed + 7919)
+    sigma = scn.spec.noise_fraction * float(np.sqrt(np.mean(y ** 2)))
+    scn.measurements = (y + rng.normal(0.0, sigma, size=y.shape)).astype(np.float32)
+    cores = host_cores()
+    V, T = scn.num_voxels, scn.num_steps
+    seg = max(1, T // max(1, args.steps))
     for _ in range(args.warmup):
-        pass  # the CPU path has no warm-up effects worth a full sample; warm-up steps are not run
-    # per-step sample sized so K steps stay within a few minutes
-    per_step = max(20, min(args.cpu_steps, (10 * scn.num_steps) // max(1, args.steps * 10)))
-    vals = []
-    t_all = 0.0
-    for _ in range(args.steps):
-        v, dt = cpu_sample(scn, per_step, threads=cores)
-        vals.append(v)
-        t_all += dt
-    value = statistics.median(vals)
+        cpu_epoch_time(scn, cores, steps=seg)
+    total = cpu_epoch_time(scn, cores)
+    value = 1.0 / total
+    one_steps = max(1, T // 5)
+    one = cpu_epoch_time(scn, 1, steps=one_steps)
+    one_all = cpu_epoch_time(scn, cores, steps=one_steps)
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -203,18 +210,24 @@ def reference_arm(args):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": 1000.0 / value,
+        "ms_per_step": 1000.0 * total / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded)",
-        "config": {"workload": f"{args.workload}: 20x20x20 cuboid, 24000 states, T=2000, 111 sensor rows, 1 beat, "
-                               "Adam lr 1e-3, gains+coefficients", "parallelism": f"{cores} CPU threads, one scenario each"},
+        "config": {"workload": f"{args.workload}: 20x20x20 cuboid, {V} voxels, {3 * V} states, T={T}, "
+                               f"{scn.num_sensors} sensor rows, 1 beat, 1 % noise, Adam lr 1e-3, gains+coefficients",
+                   "parallelism": f"{cores} host threads (OpenMP over independent outputs)",
+                   "step": f"time steps [k T/K, (k+1) T/K) of one epoch ({seg} of {T})"},
+        "voxel_steps_per_s": value * V * T,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"first {per_step} of {scn.num_steps} steps of one epoch per thread, scaled by "
-                                   f"{scn.num_steps / per_step:.0f}; later steps are slower on x86 (subnormal states), so "
-                                   "this overstates CPU throughput"},
+                         "sample": f"one full {T}-step epoch ({total:.1f} s) timed as {args.steps} steps; "
+                                   f"{args.warmup} warm-up runs of the first {seg} time steps",
+                         "single_thread_sample": {
+                             "seconds": one, "cores": 1, "threads_speedup_on_sample": one / one_all,
+                             "sample": f"first {one_steps} of {T} time steps (before states decay to subnormal "
+                                       f"values; the full all-core epoch above includes the slower later steps)"}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -224,18 +237,23 @@ def reference_arm(args):
 # ----------------------------------------------------------------------------------------- GPU
 
 
-def profiled_traffic(phase, workload):
-    """DRAM bytes per launch of the phase's kernel, from the committed ncu summary of this workload
-    (the forward phase runs the resident form when every tile fits a co-resident CTA, as on cuboid20)."""
+def profiled_counters(kernel, workload):
+    """Per-launch ncu figures of `kernel` on `workload` from its committed summary
+    (profiles/<kernel>_<workload>.md): DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum), warp
+    instructions, and the capture date and file, or None where the summary lacks them."""
     import re
 
-    for kernel in {"forward": ("forward_ring_kernel", "forward_stream_kernel"), "derive": ("derive_kernel",)}.get(phase, ()):
-        path = ROOT / "profiles" / f"{kernel}_{workload}.md"
-        if path.exists():
-            m = re.search(r"^traffic_bytes_per_launch:\s*(\d+)", path.read_text(), re.M)
-            if m:
-                return int(m.group(1))
-    return None
+    path = ROOT / "profiles" / f"{kernel}_{workload}.md"
+    if not path.exists():
+        return None
+    text = path.read_text()
+    out = {"file": f"profiles/{path.name}"}
+    for key, pat in (("traffic", r"^traffic_bytes_per_launch:\s*(\d+)"),
+                     ("instructions", r"^warp_instructions_per_launch:\s*(\d+)"),
+                     ("date", r"^captured:\s*(\S+)")):
+        m = re.search(pat, text, re.M)
+        out[key] = (int(m.group(1)) if key != "date" else m.group(1)) if m else None
+    return out
 
 
 def timed_epochs(stream, run, n, flush=None):
@@ -431,14 +449,22 @@ def batch_precision_check(alg, sc, ctx, specs, work, prec):
     return out
 
 
-def batched_section(args, alg, sc, ctx, prec, stream, flush):
+def batched_section(args, alg, sc, ctx, prec, stream, flush, rank=0, world=1):
     """64 scenarios of uneven size (batch_workload_specs): the batched adjoint epoch (one forward and
     one adjoint launch per beat index over every member, replayed from a CUDA graph) against the plain
-    one-scenario GPU form run over every member in turn."""
+    one-scenario GPU form run over every member in turn, and against the persistent one-scenario
+    adjoint epoch (ct_run_epoch) run over every member in turn. With N ranks the scenarios are split
+    by a greedy balance of voxel-steps (replicas.shard_scenarios), each rank batches its share, and
+    every time is the max over ranks; no collective touches the data path."""
     import numpy as np
 
+    from cardiotrust_b200 import replicas
+
     t0 = time.perf_counter()
-    specs = sc.batch_workload_specs(args.batch_scenarios, seed=0)
+    all_specs = sc.batch_workload_specs(args.batch_scenarios, seed=0)
+    costs = [replicas.scenario_cost(sc.voxel_count(sp), sp.num_steps, sp.num_beats) for sp in all_specs]
+    mine = replicas.shard_scenarios(costs, world)[rank]
+    specs = [all_specs[i] for i in mine]
     cfg = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False,
                         ap_derivative=alg.APDerivative.Textbook)
     engines, vtb, sizes, vtbs = [], 0, [], []
@@ -463,25 +489,36 @@ def batched_section(args, alg, sc, ctx, prec, stream, flush):
     batch.run_epoch(sync=True)
     phases = {k: v for k, v in batch.read_profile().items() if v > 0}
     batch.set_profiling(False)
-    chosen_ms = statistics.mean(ms)
-    n = len(engines)
-    # plain one-scenario form over every member, one epoch each (after one warm-up epoch of the smallest)
+    chosen_ms = replicas.max_over_ranks(statistics.mean(ms))
+    n = len(all_specs)
+    vtb = int(replicas.sum_over_ranks(vtb))
+    # the persistent one-scenario adjoint epoch (ct_run_epoch) over every member in turn, same products
     small = int(np.argmin(sizes))
+    engines[small].run_epoch(0, grad_mode=alg.GradMode.Adjoint, precision=prec, sync=True)
+    seq_ms = 0.0
+    for e in engines:
+        seq_ms += timed_epochs(stream, lambda: e.run_epoch(0, grad_mode=alg.GradMode.Adjoint, precision=prec,
+                                                             sync=False), 1, flush)[0]
+    seq_ms = replicas.max_over_ranks(seq_ms)
+    # plain one-scenario form over every member, one epoch each (after one warm-up epoch of the smallest)
     engines[small].run_epoch_plain(0, sync=True)
     plain_ms = 0.0
     for k, e in enumerate(engines):
         plain_ms += timed_epochs(stream, lambda: e.run_epoch_plain(0, sync=False), 1)[0]
+    plain_ms = replicas.max_over_ranks(plain_ms)
     batch.close()
     for e in engines:
         e.close()
-    check = batch_precision_check(alg, sc, ctx, specs, vtbs, prec)
+    check = batch_precision_check(alg, sc, ctx, specs, vtbs, prec) if world == 1 else None
     chosen = n * 1000.0 / chosen_ms
     plain = n * 1000.0 / plain_ms
+    seq = n * 1000.0 / seq_ms
     return {
         "workload": f"{n} scenarios: voxels log-uniform 500..30000 (cuboids and shells), 1-8 beats, 1000-4000 "
                     "steps, 37-128 triaxial sensors, random 3^3 pathological block and pulse onset, Adam lr 1e-3, "
                     "gains+coefficients",
-        "scenarios": n, "voxels_total": int(sum(sizes)), "voxel_steps_per_epoch": int(vtb),
+        "scenarios": n, "ranks": world, "scenarios_this_rank": len(specs),
+        "voxels_total_this_rank": int(sum(sizes)), "voxel_steps_per_epoch": int(vtb),
         "build_s": build_s,
         "chosen": {"form": "batched: one persistent forward and one persistent adjoint launch per beat index over "
                            "every member's tiles, epoch replayed from a CUDA graph; adjoint gradients, checkpoint interval "
@@ -493,7 +530,11 @@ def batched_section(args, alg, sc, ctx, prec, stream, flush):
         "plain": {"form": "plain GPU form, one scenario at a time, one launch per phase per step (reference "
                           "gradients, FP32)", "scenario_epochs_per_s": plain,
                   "voxel_steps_per_s": vtb * 1000.0 / plain_ms, "ms_per_epoch_all": plain_ms},
+        "sequential_persistent": {"form": "the persistent one-scenario adjoint epoch (ct_run_epoch), one member "
+                                          "after another, same products", "scenario_epochs_per_s": seq,
+                                  "voxel_steps_per_s": vtb * 1000.0 / seq_ms, "ms_per_epoch_all": seq_ms},
         "chosen_vs_plain": chosen / plain,
+        "chosen_vs_sequential_persistent": chosen / seq,
         "gradient_error": check,
     }
 
@@ -715,27 +756,46 @@ def gpu_arm(args):
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     S = 3 * V
     phase_ms = {k: v[0] / args.steps for k, v in prof.items()}
-    dominant = max(phase_ms, key=phase_ms.get)
-    # algorithmic bytes per launch (per beat): propagation 601*S per step; derivative sweep 740*S per step
-    algo_bytes = {"forward": 601.0 * S * T, "derive": 740.0 * S * T}
-    rl_kernel = dominant if dominant in algo_bytes else "forward"
-    launches_of = max(1, prof[rl_kernel][1] // args.steps)
-    per_launch_ms = phase_ms[rl_kernel] / launches_of
-    achieved = algo_bytes[rl_kernel] / (per_launch_ms / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": rl_kernel, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+    # the dominant kernel of the epoch is the forward propagation (one launch per beat)
+    launches_of = max(1, prof["forward"][1] // args.steps)
+    per_launch_ms = phase_ms["forward"] / launches_of
+    # the resident form runs when every 32-voxel tile fits a co-resident CTA (two per SM)
+    fwd_kernel = "forward_ring_kernel" if (V + 31) // 32 <= 2 * 148 else "forward_stream_kernel"
+    # bytes a launch must move through HBM in this design: the state history it writes (4 B per
+    # state-step), and once per launch the gains [S,78], coefficients, delays and neighbour table
+    # [V,26], the all-pass state [V,78] read and written, control column and function
+    must = 4.0 * S * T + 4.0 * 78 * S + 12.0 * 26 * V + 2 * 4.0 * 78 * V + 4.0 * S + 4.0 * T
+    achieved = must / (per_launch_ms / 1000.0) / 1e9
+    pc = profiled_counters(fwd_kernel, args.workload) or {}
+    sm_mhz = (clock or {}).get("sm_mhz") or 1965.0
+    issue = None
+    if pc.get("instructions"):
+        issue = pc["instructions"] / (148 * 4 * sm_mhz * 1e6 * per_launch_ms / 1000.0)
+    roofline = {"bound": "hbm", "kernel": fwd_kernel, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "peak_source": peak_src,
-                "traffic": profiled_traffic(rl_kernel, args.workload),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch (profiles/)",
-                "algorithmic_bytes_per_launch": algo_bytes[rl_kernel], "launch_ms": per_launch_ms}
+                "traffic": pc.get("traffic"),
+                "traffic_source": (f"{pc['file']} (ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                                   f"captured {pc.get('date')})") if pc else None,
+                "algorithmic_bytes_per_launch": must,
+                "algorithmic_model": "state history written once (4 B per state-step) + per-launch parameters "
+                                     "and all-pass state; neighbour history, gains and chain state stay on chip",
+                "launch_ms": per_launch_ms,
+                "limiter": "issue and latency, not HBM: warp-instruction issue over the SMs' 4 schedulers at the "
+                           "median SM clock is `issue_utilisation`; the step recurrence serialises time",
+                "issue_utilisation": issue,
+                "reference_layout_throughput": {
+                    "bytes_per_state_step": 601, "GB_per_s": 601.0 * S * T / (per_launch_ms / 1000.0) / 1e9,
+                    "note": "the reference's per-step reads (gains, all-pass state, coefficients, history every step) "
+                            "over the launch time: a throughput figure, not HBM traffic"}}
 
     # ---- plain GPU form and adjoint mode on the same workload; the batched workload. The plain forms
     # are launch-bound, so nothing else runs on the host while they are timed.
     forms = forms_section(alg, eng, bi, prec, stream, flush, scn)
     post_run = post_run_section(alg, eng, scn, stream, hbm_peak, prec)
     batched = None
-    if args.batch_scenarios > 0 and world == 1:
+    if args.batch_scenarios > 0:
         eng.close()
-        batched = batched_section(args, alg, sc, ctx, prec, stream, flush)
+        batched = batched_section(args, alg, sc, ctx, prec, stream, flush, rank, world)
 
     # ---- precision report: the f64 oracle on the host, then the GPU products of the same cases
     precision = None
@@ -744,18 +804,18 @@ def gpu_arm(args):
         prec_job.start()
         precision = precision_section(alg, ctx, prec_job)
 
-    # ---- CPU baseline (rank 0, N = 1 only)
+    # ---- CPU baseline (rank 0, N = 1 only): one full epoch of the CPU restatement on every host core
     cpu = None
     if rank == 0 and world == 1:
         try:
             import oracle
 
             oracle.build()
-            v, dt = cpu_sample(scn, args.cpu_steps, threads=1)
-            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                   "sample": f"first {min(args.cpu_steps, T)} of {T} steps of one epoch (single thread, reference "
-                             f"loop order), scaled by {T / min(args.cpu_steps, T):.0f}; {dt:.1f} s; later steps are "
-                             "slower on x86 (subnormal states), so this overstates CPU throughput"}
+            cores = host_cores()
+            dt = cpu_epoch_time(scn, cores)
+            cpu = {"value": 1.0 / dt, "unit": UNIT, "cores": cores, "kind": "port",
+                   "sample": f"one full {T}-step epoch of the workload ({dt:.1f} s), f32 restatement in the "
+                             "reference's loop order, OpenMP over independent outputs (bit-identical to one thread)"}
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "port", "sample": f"failed: {exc}"}
 
@@ -771,7 +831,8 @@ def gpu_arm(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32",
+            "dtype": {"fp32": "f32", "tf32x3": "f32 (products tf32x3)", "tf32": "f32 (products tf32)",
+                      "bf16x6": "f32 (products bf16x6: BF16 slices, exact FP32 accumulation)"}[args.precision],
             "data": "synthetic (seeded)",
             "config": {
                 "workload": f"{args.workload}: 20x20x20 cuboid, {V} voxels, {S} states, T={T}, "

@@ -44,6 +44,10 @@ struct ct_scn {
   ct_algorithm algo{};
   DeviceScenario d{};
   int64_t adam_step = 1;  // Derivatives.step, derivation.rs:100
+  // TF32 product modes (index 0: CT_PREC_TF32X3, 1: CT_PREC_TF32): 0 unchecked, 1 accepted, -1 refused,
+  // and the relative gradient difference the check measured
+  int tf32_verdict[2] = {0, 0};
+  double tf32_rel[2] = {0.0, 0.0};
   uint64_t rng = 0x9e3779b97f4a7c15ull;
   std::vector<void*> allocations;
   std::vector<int32_t> nbr_host;  // neighbour table in reference order, for validating delay writes
@@ -572,13 +576,16 @@ void scatter_state_columns(float* dst, const float* src, const std::vector<int32
 // (voxel, offset) items read, and each item's slot in that list. False if a neighbourhood
 // exceeds kFwdHaloMax (the resident forward form is then not used).
 bool build_halos(const ct_scn* s, const std::vector<int32_t>& nbr_ref, int64_t tiles, std::vector<int32_t>& halo,
-                 std::vector<int32_t>& nhalo, std::vector<int16_t>& hslot) {
-  const int TV = ct::kFwdTileVoxels, HM = ct::kFwdHaloMax;
+                 std::vector<int32_t>& nhalo, std::vector<int16_t>& hslot, std::vector<int32_t>& nbt,
+                 std::vector<int32_t>& nnbt) {
+  const int TV = ct::kFwdTileVoxels, HM = ct::kFwdHaloMax, NT = ct::kFwdNbTilesMax;
   const int64_t V = (int64_t)s->perm.size();
   halo.assign((size_t)(tiles * HM), -1);
   nhalo.assign((size_t)tiles, 0);
   hslot.assign((size_t)(tiles * TV * kOffsets), -1);
-  std::vector<int32_t> list;
+  nbt.assign((size_t)(tiles * NT), -1);
+  nnbt.assign((size_t)tiles, 0);
+  std::vector<int32_t> list, owners;
   for (int64_t t = 0; t < tiles; ++t) {
     list.clear();
     for (int vl = 0; vl < TV; ++vl) {
@@ -594,6 +601,15 @@ bool build_halos(const ct_scn* s, const std::vector<int32_t>& nbr_ref, int64_t t
     if ((int)list.size() > HM) return false;
     nhalo[(size_t)t] = (int32_t)list.size();
     std::copy(list.begin(), list.end(), halo.begin() + (size_t)(t * HM));
+    // the other tiles whose states this tile's steps read (the tiles it waits for between blocks)
+    owners.clear();
+    for (int32_t dw : list)
+      if (dw / TV != t) owners.push_back(dw / TV);
+    std::sort(owners.begin(), owners.end());
+    owners.erase(std::unique(owners.begin(), owners.end()), owners.end());
+    if ((int)owners.size() > NT) return false;
+    nnbt[(size_t)t] = (int32_t)owners.size();
+    std::copy(owners.begin(), owners.end(), nbt.begin() + (size_t)(t * NT));
     for (int vl = 0; vl < TV; ++vl) {
       const int64_t u = t * TV + vl;
       if (u >= V) break;
@@ -884,10 +900,10 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   // forward form: resident (one tile per CTA, halo ring) when every tile fits a co-resident CTA
   // and every tile's neighbourhood fits the ring; streaming otherwise
   const int64_t tiles = (d.V + ct::kFwdTileVoxels - 1) / ct::kFwdTileVoxels;
-  std::vector<int32_t> h_halo, h_nhalo;
+  std::vector<int32_t> h_halo, h_nhalo, h_nbt, h_nnbt;
   std::vector<int16_t> h_hslot;
   d.fwd_ring = tiles <= ct::forward_ring_capacity(ctx->device) &&
-               build_halos(s, nbr, tiles, h_halo, h_nhalo, h_hslot);
+               build_halos(s, nbr, tiles, h_halo, h_nhalo, h_hslot, h_nbt, h_nnbt);
   d.fwd_grid = d.fwd_ring ? (int)tiles : ct::forward_grid_size(d.V, ctx->device);
   {
     const int64_t tiles = ((M + 63) / 64) * ((T + 63) / 64);
@@ -964,6 +980,9 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
     ALLOC(d.halo, tiles * ct::kFwdHaloMax);
     ALLOC(d.hslot, tiles * ct::kFwdTileVoxels * kOffsets);
     ALLOC(d.nhalo, tiles);
+    ALLOC(d.nbt, tiles * ct::kFwdNbTilesMax);
+    ALLOC(d.nnbt, tiles);
+    ALLOC(d.progress, tiles);
   }
   ALLOC(d.status, 1);
   ALLOC(d.barrier, 1);
@@ -998,6 +1017,8 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
     r = r ? r : upload(s, d.halo, h_halo.data(), sizeof(int32_t) * h_halo.size());
     r = r ? r : upload(s, d.hslot, h_hslot.data(), sizeof(int16_t) * h_hslot.size());
     r = r ? r : upload(s, d.nhalo, h_nhalo.data(), sizeof(int32_t) * h_nhalo.size());
+    r = r ? r : upload(s, d.nbt, h_nbt.data(), sizeof(int32_t) * h_nbt.size());
+    r = r ? r : upload(s, d.nnbt, h_nnbt.data(), sizeof(int32_t) * h_nnbt.size());
   }
   r = r ? r : upload(s, d.u, desc->control_function, sizeof(float) * T);
   if (!r && desc->measurements) r = upload(s, d.meas, desc->measurements, sizeof(float) * B * T * M);
@@ -1100,6 +1121,61 @@ static int run_beat_plain(ct_scn* s, int64_t beat) {
   return CT_OK;
 }
 
+// The TF32 product modes accumulate with a bias (the tensor core's FP32 adds are not round-to-nearest)
+// that the gradient, a near-cancelling sum of residual terms, does not average out when the residuals
+// are a small fraction of the signal. Before a scenario's first epoch in such a mode, the first beat's
+// reference-mode gradients are computed with the mode and with the sliced BF16 products (unbiased, within
+// ~1e-4 of FP64); if they differ by more than the 1e-3 gradient target (norm-wise), the mode is refused for
+// this scenario. The check leaves parameters, Adam state and the batch cursor untouched; it overwrites
+// the estimation outputs of the last epoch (states, predicted measurements, residuals, step metrics).
+constexpr double kTf32GradientBar = 1e-3;
+
+int check_tf32_gradients(ct_scn* s, int precision) {
+  const int slot = precision == CT_PREC_TF32 ? 1 : 0;
+  if (s->tf32_verdict[slot] > 0) return CT_OK;
+  if (s->tf32_verdict[slot] < 0)
+    return fail(CT_ERR_NOT_SUPPORTED,
+                "precision %d refused for this scenario: its first-beat gradients differ by %.2e (norm-wise) from "
+                "the sliced BF16 products' (bar %.0e); use CT_PREC_BF16X6 or CT_PREC_FP32",
+                precision, s->tf32_rel[slot], kTf32GradientBar);
+  const ct_algorithm& a = s->algo;
+  if (a.freeze_gains && a.freeze_delays) return CT_OK;  // no gradients to compare
+  int rc = prepare_sliced(s);
+  if (rc) return rc;
+  DeviceScenario& d = s->d;
+  const bool prof = s->profiling;
+  s->profiling = false;
+  std::vector<float> g[2], c[2];
+  for (int pass = 0; pass < 2 && !rc; ++pass) {
+    rc = derivatives_reset(s);
+    if (!rc) rc = run_beat(s, 0, pass == 0 ? precision : CT_PREC_BF16X6, CT_GRAD_REFERENCE);
+    if (!rc) {
+      g[pass].resize((size_t)(d.S * kGainCols));
+      c[pass].resize((size_t)(d.V * kOffsets));
+      rc = copy_down(s, g[pass].data(), d.dG, sizeof(float) * g[pass].size());
+      if (!rc) rc = copy_down(s, c[pass].data(), d.dC, sizeof(float) * c[pass].size());
+    }
+  }
+  s->profiling = prof;
+  if (!rc) rc = derivatives_reset(s);
+  if (rc) return rc;
+  auto rel = [](const std::vector<float>& x, const std::vector<float>& y) {
+    double num = 0.0, den = 0.0;
+    for (size_t i = 0; i < x.size(); ++i) {
+      const double e = (double)x[i] - (double)y[i];
+      num += e * e;
+      den += (double)y[i] * (double)y[i];
+    }
+    return den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
+  };
+  const double eg = a.freeze_gains ? 0.0 : rel(g[0], g[1]);
+  const double ec = a.freeze_delays ? 0.0 : rel(c[0], c[1]);
+  const double e = std::max(eg, ec);
+  s->tf32_rel[slot] = e;
+  s->tf32_verdict[slot] = (e <= kTf32GradientBar) ? 1 : -1;
+  return check_tf32_gradients(s, precision);
+}
+
 static int run_epoch_impl(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, int grad_mode,
                           int precision, bool plain) {
   if (!scn || !batch_index) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
@@ -1112,6 +1188,10 @@ static int run_epoch_impl(ct_scn* scn, int64_t* batch_index, const int32_t* beat
   CT_DEVICE_SCOPE(scn->ctx->device);
   if (precision == CT_PREC_BF16X6 && !plain) {
     int rc0 = prepare_sliced(scn);
+    if (rc0) return rc0;
+  }
+  if ((precision == CT_PREC_TF32X3 || precision == CT_PREC_TF32) && !plain) {
+    int rc0 = check_tf32_gradients(scn, precision);
     if (rc0) return rc0;
   }
   DeviceScenario& d = scn->d;
@@ -1838,6 +1918,12 @@ int ct_batch_create(ct_ctx* ctx, ct_scn* const* scenarios, int64_t count, int gr
     for (int64_t i = 0; i < count; ++i)
       if (scenarios[i]->d.umma) {
         int rc0 = prepare_sliced(scenarios[i]);
+        if (rc0) return rc0;
+      }
+  if (precision == CT_PREC_TF32X3 || precision == CT_PREC_TF32)  // the members' gradient check
+    for (int64_t i = 0; i < count; ++i)
+      if (scenarios[i]->d.umma) {
+        int rc0 = check_tf32_gradients(scenarios[i], precision);
         if (rc0) return rc0;
       }
   ct_batch* b = new ct_batch;

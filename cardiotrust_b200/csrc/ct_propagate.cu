@@ -13,8 +13,11 @@
 //     cooperative grid walks the tiles.
 //   * Every read of the recurrence is of x[t-d] or x[t-d-1] with d >= 1, so
 //     the states of steps t .. t+L-1 are independent when L <= min delay.
-//     The kernel advances L = min(dmin, kMaxStepBlock) steps between two grid
-//     barriers (monotone counter, ct_sync.cuh).
+//     The kernel advances L = min(dmin, kMaxStepBlock) steps between two
+//     synchronisations: a grid barrier (monotone counter, ct_sync.cuh) in the
+//     streaming forms; in the resident form each tile publishes the blocks it
+//     has completed and waits only for the tiles its neighbourhood reads from
+//     (tile_wait, ct_sync.cuh), so no CTA waits for the slowest of the grid.
 //   * The all-pass state is deduplicated: ap_outputs[3v+a, 3n+b] does not
 //     depend on the row component a (same input state, coefficient and zero
 //     start, prediction.rs:56-79), so it is kept as [V, 26*3].
@@ -39,8 +42,8 @@
 //     per (voxel, offset), the chain state, and the round buffers. A CTA that
 //     owns one tile stages it once per launch.
 //   * History reads go through L1: within one launch a history row is read
-//     only after the grid barrier that completes it, so no SM can hold a
-//     stale line of it (L1 holds no global data across launches).
+//     only after the acquire (grid barrier or neighbour progress) that orders
+//     its writes before the read.
 #include <cuda_runtime.h>
 
 #include "ct_internal.cuh"
@@ -500,6 +503,9 @@ struct RingArgs {
   const int32_t* halo;    // [tiles, kHaloMax], -1 padded
   const int16_t* hslot;   // [tiles, kTileItems], halo slot of the item's neighbour, -1 if absent
   const int32_t* nhalo;   // [tiles]
+  const int32_t* nbt;     // [tiles, kFwdNbTilesMax] other tiles the tile's steps read from
+  const int32_t* nnbt;    // [tiles]
+  unsigned int* progress; // [tiles] blocks completed, zeroed before the launch
 };
 
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
@@ -511,19 +517,24 @@ __device__ __forceinline__ void cp_async_commit_wait_all() {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 
+// Producer p stages the ring columns q = p + kProducers * i (i < kStageSlots) of every history row;
+// col[i] is the state index 3 * halo[q / 3] + q % 3 of column q, or -1 beyond the halo's 3 nh columns
+// (computed once per launch, so a staged element costs an address add and the copy).
+constexpr int kStageSlots = (kHaloMax * 3 + kProducers - 1) / kProducers;
+
 // Producers: copy history rows [r_lo, r_hi] of the halo into the ring (rows before t = 0 are zero).
-__device__ __forceinline__ void stage_rows(RingSmem& sm, const FwdArgs& p, int nh, int r_lo, int r_hi) {
-  const int per_row = 3 * nh;
-  const int total = (r_hi - r_lo + 1) * per_row;
-  for (int f = threadIdx.x; f < total; f += kProducers) {
-    const int rr = f / per_row, rem = f - rr * per_row;
-    const int row = r_lo + rr;
-    float* dst = &sm.ring[row & (kRingRows - 1)][rem];
-    if (row < 0) {
-      *dst = 0.0f;
-    } else {
-      const int hv = rem / 3, b = rem - 3 * (rem / 3);
-      cp_async4(dst, p.X + (size_t)row * p.S + 3 * sm.halo[hv] + b);
+__device__ __forceinline__ void stage_rows(RingSmem& sm, const FwdArgs& p, const int (&col)[kStageSlots], int r_lo,
+                                           int r_hi) {
+  for (int row = r_lo; row <= r_hi; ++row) {
+    float* dst = sm.ring[row & (kRingRows - 1)] + threadIdx.x;
+    const float* src = p.X + (size_t)(row < 0 ? 0 : row) * p.S;
+#pragma unroll
+    for (int i = 0; i < kStageSlots; ++i) {
+      if (col[i] < 0) continue;
+      if (row < 0)
+        dst[i * kProducers] = 0.0f;
+      else
+        cp_async4(dst + i * kProducers, src + col[i]);
     }
   }
 }
@@ -588,9 +599,15 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
     }
   }
   __syncthreads();
+  int stage_col[kStageSlots];
+#pragma unroll
+  for (int i = 0; i < kStageSlots; ++i) {
+    const int q = threadIdx.x + i * kProducers;
+    stage_col[i] = (producer && q < 3 * nh) ? 3 * sm.halo[q / 3] + q % 3 : -1;
+  }
 
   int round = 0;
-  unsigned int barrier_number = 0;
+  unsigned int blocks_done = 0;
   int staged_top = -dmin - 1 + kRound - 1 - kRound;  // highest ring row staged so far (none)
 
   for (int t0 = 0; t0 < T; t0 += Lmax) {
@@ -607,7 +624,7 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
           if (r0 == 0) {
             const int top_blk = t0 + L - 1 - dmin;  // newest history row the block reads
             if (top_blk > staged_top) {
-              stage_rows(sm, p, nh, staged_top + 1, top_blk);
+              stage_rows(sm, p, stage_col, staged_top + 1, top_blk);
               staged_top = top_blk;
             }
             cp_async_commit_wait_all();
@@ -615,7 +632,7 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
           }
         } else if (use_ring) {
           if (r0 == 0 && top > staged_top) {  // first round of a block: rows produced in the previous block
-            stage_rows(sm, p, nh, staged_top + 1, top);
+            stage_rows(sm, p, stage_col, staged_top + 1, top);
             staged_top = top;
           }
           cp_async_commit_wait_all();
@@ -626,7 +643,7 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
             const int Rn = (L - r0n) < kRound ? (L - r0n) : kRound;
             const int topn = t0 + r0n + Rn - 1 - dmin;
             if (topn > staged_top) {
-              stage_rows(sm, p, nh, staged_top + 1, topn);
+              stage_rows(sm, p, stage_col, staged_top + 1, topn);
               staged_top = topn;
             }
           }
@@ -772,7 +789,11 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
     __syncthreads();
     if ((int)threadIdx.x < L) p.stepsum_part[(size_t)(t0 + threadIdx.x) * gridDim.x + blockIdx.x] = sm.part[threadIdx.x];
     if (t0 + L < T) {
-      if (!grid_barrier(p.barrier, barrier_number++, p.status)) {
+      // the next block reads rows at least dmin >= L steps old: only the tiles of this tile's
+      // neighbourhood must have completed the current block
+      ++blocks_done;
+      if (!tile_wait(ra.progress, tile, blocks_done, ra.nbt + (size_t)tile * kFwdNbTilesMax, ra.nnbt[tile],
+                     p.status)) {
         if (producer) cp_async_commit_wait_all();
         return;
       }
@@ -874,10 +895,15 @@ cudaError_t launch_forward(DeviceScenario& d, float threshold, float* ckpt, cuda
   err = cudaMemsetAsync(d.barrier, 0, sizeof(GridBarrier), stream);
   if (err != cudaSuccess) return err;
   if (d.fwd_ring) {
+    err = cudaMemsetAsync(d.progress, 0, sizeof(unsigned int) * (size_t)d.fwd_grid, stream);
+    if (err != cudaSuccess) return err;
     RingArgs r;
     r.halo = d.halo;
     r.hslot = d.hslot;
     r.nhalo = d.nhalo;
+    r.nbt = d.nbt;
+    r.nnbt = d.nnbt;
+    r.progress = d.progress;
     void* args[] = {&a, &r};
     return launch_cooperative((const void*)forward_ring_kernel, d.fwd_grid, kThreads, args, sizeof(RingSmem), stream);
   }

@@ -437,8 +437,11 @@ cudaError_t launch_measure_sliced(DeviceScenario& d, int64_t beat, bool with_res
     return cudaErrorInvalidValue;
   const int kchunks = (int)(sp / kChunk);
   const int groups = (int)ngs;
-  const int ks = d.ksplit_slice;
-  const int per = ((groups + ks - 1) / ks) * kGroupChunks;
+  // whole groups per split; every split of the grid has at least one group, and the reduction
+  // below sums exactly the splits the grid writes (ks <= d.ksplit_slice, the partial buffer's count)
+  const int per_groups = (groups + d.ksplit_slice - 1) / d.ksplit_slice;
+  const int ks = (groups + per_groups - 1) / per_groups;
+  const int per = per_groups * kGroupChunks;
   const int ldp = (int)(((M + 127) / 128) * 128);
   e = launch_slice_gemm<128>(ma, mb, d.X_sc, d.H_sc + beat * M * ngs, (int)ngs, d.gemm_part, ldp,
                              (long long)T * ldp, (int)T, (int)M, kchunks, per, ks, d.status, stream);

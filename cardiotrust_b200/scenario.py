@@ -201,6 +201,11 @@ def _mask(spec: ScenarioSpec) -> np.ndarray:
     raise ValueError(f"unknown mask {spec.mask!r}")
 
 
+def voxel_count(spec: ScenarioSpec) -> int:
+    """Voxels of the scenario a spec builds (the mask's cells), without building it."""
+    return int(_mask(spec).sum())
+
+
 def _positions(shape, size_mm: float) -> np.ndarray:
     """Voxel centres: size*idx + size/2 (voxels.rs:499-527, zero heart offset)."""
     nx, ny, nz = shape

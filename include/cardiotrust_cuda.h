@@ -75,13 +75,20 @@ enum ct_precision {
   CT_PREC_FP32 = 0,   /* FP32 CUDA-core GEMMs */
   CT_PREC_TF32X3 = 1, /* tcgen05 TF32 with a hi/lo split of both operands (hi*hi + hi*lo + lo*hi), FP32
                          accumulate. The tensor core's accumulation is biased toward zero: when residuals are a
-                         small fraction of the signal, gradients drift ~1e-2 from the FP64 result. */
-  CT_PREC_TF32 = 2,   /* tcgen05 TF32, one pass (operands rounded to TF32) */
+                         small fraction of the signal, gradients drift ~1e-2 from the FP64 result. Guarded: see
+                         below. */
+  CT_PREC_TF32 = 2,   /* tcgen05 TF32, one pass (operands rounded to TF32). Guarded: see below. */
   CT_PREC_BF16X6 = 3  /* tcgen05 BF16 on error-free slices: every operand row is cut into groups of 512 values
                          sharing a power-of-two scale and split into three 8-bit integer slices (exact in BF16);
                          six slice products accumulate exactly in FP32 tensor memory and are folded into an FP32
                          sum, rounding to nearest, every 512 values. Unbiased like FP32 CUDA-core products. */
 };
+/* Guard of the TF32 modes: before a scenario's first epoch in CT_PREC_TF32X3 or CT_PREC_TF32 (ct_run_epoch,
+ * ct_run_model_based, ct_batch_create), the first beat's reference-mode gradients are computed with the mode and
+ * with CT_PREC_BF16X6. If they differ by more than 1e-3 (norm-wise relative, the gradient target), the call
+ * returns CT_ERR_NOT_SUPPORTED with the measured difference in ct_last_error, and every later call in that mode
+ * on that scenario does too. Parameters, derivatives, Adam state and the batch cursor are left untouched; the
+ * last epoch's estimation outputs (states, predicted measurements, residuals, step metrics) are overwritten. */
 
 /* The Algorithm fields the epoch reads, src/core/config/algorithm.rs:25-58. */
 typedef struct ct_algorithm {

@@ -83,3 +83,26 @@ def test_gradients_meet_bar_on_768_row_shell(shell768, precision):
     assert errs["measurements"] < 1e-5, errs
     for k in ("grad_gains", "grad_coefs", "adjoint_grad_gains", "adjoint_grad_coefs"):
         assert errs[k] < TOL_GRAD, (precision, errs)
+
+
+def test_tf32x3_refused_on_768_row_shell(shell768):
+    """The TF32 split products' biased accumulation fails the gradient target here: the library refuses the
+    mode (CT_ERR_NOT_SUPPORTED, parameters and derivatives untouched) instead of returning 2e-2 gradients."""
+    from cardiotrust_b200 import _lib
+    from cardiotrust_b200 import algorithm as alg
+
+    scn, _ = shell768
+    ctx = alg.Context(0)
+    cfg = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
+    eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=cfg)
+    g0, c0 = eng.read("gains"), eng.read("coefs")
+    for _ in range(2):  # the verdict is kept: the second call refuses without re-checking
+        with pytest.raises(_lib.CtError) as exc:
+            eng.run_epoch(0, precision=alg.Precision.Tf32x3)
+        assert exc.value.status == _lib.CT_ERR_NOT_SUPPORTED
+        assert "refused" in str(exc.value)
+    assert np.array_equal(eng.read("gains"), g0) and np.array_equal(eng.read("coefs"), c0)
+    assert not np.any(eng.read("grad_gains"))
+    eng.run_epoch(0, precision=alg.Precision.Bf16x6)  # the sliced products run on the same scenario
+    eng.close()
+    ctx.close()
