@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--batch-scenarios", type=int, default=64,
                    help="scenarios of the batched section (0 skips it)")
     p.add_argument("--batch-epochs", type=int, default=3, help="timed epochs of the batched section")
+    p.add_argument("--cpu-baseline", type=int, default=1, help="time the CPU restatement's full epoch (0 skips it)")
     p.add_argument("--precision-steps", type=int, default=48,
                    help="steps of the precision report (shell, 256 triaxial sensors) against the f64 oracle (0 skips)")
     return p.parse_args()
@@ -806,7 +807,7 @@ def gpu_arm(args):
 
     # ---- CPU baseline (rank 0, N = 1 only): one full epoch of the CPU restatement on every host core
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_baseline:
         try:
             import oracle
 
