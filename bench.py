@@ -607,11 +607,18 @@ def precision_case(alg, ctx, scn, ref):
         b = np.asarray(b, np.float64)
         return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
+    from cardiotrust_b200 import _lib
+
     results = {}
     for name, prec in (("fp32", alg.Precision.Fp32), ("tf32x3", alg.Precision.Tf32x3), ("tf32", alg.Precision.Tf32),
                        ("bf16x6", alg.Precision.Bf16x6)):
         eng = alg.EpochEngine.from_scenario(ctx, scn, algorithm=cfg)
-        eng.run_epoch(0, beat_order=np.arange(scn.num_beats), precision=prec)
+        try:
+            eng.run_epoch(0, beat_order=np.arange(scn.num_beats), precision=prec)
+        except _lib.CtError as exc:  # the library's guard of the TF32 modes
+            eng.close()
+            results[name] = {"refused": str(exc)}
+            continue
         r = {f: rel(eng.read(f), ref[f]) for f in ("system_states", "measurements", "residuals", "grad_gains",
                                                    "grad_coefs")}
         eng.close()
