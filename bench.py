@@ -52,7 +52,7 @@ def parse():
                    help="scenarios of the batched section (0 skips it)")
     p.add_argument("--batch-epochs", type=int, default=3, help="timed epochs of the batched section")
     p.add_argument("--cpu-baseline", type=int, default=1, help="time the CPU restatement's full epoch (0 skips it)")
-    p.add_argument("--precision-steps", type=int, default=48,
+    p.add_argument("--precision-steps", type=int, default=256,
                    help="steps of the precision report (shell, 256 triaxial sensors) against the f64 oracle (0 skips)")
     return p.parse_args()
 

@@ -61,30 +61,22 @@ __global__ void __launch_bounds__(128) derive_kernel(DeriveArgs p) {
   const float dx4 = dx2 * dx2;
   const float dr_dd = p.s.diffreg * (dx * dx4);
 
-  // Lanes b = 0, 1 of every (a, b) quantity are packed in a float2 and stepped with the packed FP32
-  // instructions (fma2 / mul2 / add2 / sub2: each lane rounded to nearest like the scalar operation);
-  // lane b = 2 stays scalar. The dC sum is accumulated term by term in the reference's (a, b) order.
-  float2 g01[3], dG01[3];
-  float g2[3], dG2[3];
+  float g[3][3], dG[3][3];
+  float ap[3] = {0.0f, 0.0f, 0.0f}, fir[3], iir[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float* gr = p.gains + (3 * v + a) * kGainCols + 3 * n;
-    const float* dr = p.dG + (3 * v + a) * kGainCols + 3 * n;
-    g01[a] = make_float2(gr[0], gr[1]);
-    g2[a] = gr[2];
-    dG01[a] = make_float2(dr[0], dr[1]);
-    dG2[a] = dr[2];
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      g[a][b] = p.gains[(3 * v + a) * kGainCols + 3 * n + b];
+      dG[a][b] = p.dG[(3 * v + a) * kGainCols + 3 * n + b];
+    }
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    fir[b] = p.fir[v * kGainCols + 3 * n + b];
+    iir[b] = p.iir[v * kGainCols + 3 * n + b];
   }
-  const float* fr = p.fir + v * kGainCols + 3 * n;
-  const float* ir = p.iir + v * kGainCols + 3 * n;
-  float2 fir01 = make_float2(fr[0], fr[1]), iir01 = make_float2(ir[0], ir[1]);
-  float fir2 = fr[2], iir2 = ir[2];
-  float2 ap01 = make_float2(0.0f, 0.0f);
-  float ap2 = 0.0f;
   float dC = p.dC[idx];
   const float mse_s = p.s.mse_scaling, reg_s = p.s.reg_scaling, thr = p.s.threshold;
-  const float2 c2 = make_float2(c, c), mc2 = make_float2(minus_c, minus_c);
-  const float2 mse2 = make_float2(mse_s, mse_s), reg2 = make_float2(reg_s, reg_s), drdd2 = make_float2(dr_dd, dr_dd);
   const bool do_gains = !p.s.freeze_gains, do_coefs = !p.s.freeze_delays;
   const bool textbook = p.s.ap_derivative != 0;
 
@@ -93,8 +85,7 @@ __global__ void __launch_bounds__(128) derive_kernel(DeriveArgs p) {
   // arithmetic of step t (two-stage software pipeline).
   const float* xv = p.X + 3 * v;
   const float* mrv = p.MR + 3 * v;
-  float2 inp01 = make_float2(0.0f, 0.0f);
-  float inp2 = 0.0f;
+  float in_prev[3] = {0.0f, 0.0f, 0.0f};
   float nin[3], nx[3], nmr[3];
 #pragma unroll
   for (int b = 0; b < 3; ++b) nin[b] = (valid && d <= 0) ? __ldg(p.X + j0 + b) : 0.0f;
@@ -104,11 +95,13 @@ __global__ void __launch_bounds__(128) derive_kernel(DeriveArgs p) {
     nmr[a] = __ldg(mrv + a);
   }
   for (int64_t t = 0; t < T; ++t) {
-    const float2 in01 = make_float2(nin[0], nin[1]);
-    const float in2 = nin[2];
-    const float x0 = nx[0], x1 = nx[1], x2 = nx[2];
-    const float2 mr01 = make_float2(nmr[0], nmr[1]);
-    const float mr2 = nmr[2];
+    float in[3], x[3], mr[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      in[q] = nin[q];
+      x[q] = nx[q];
+      mr[q] = nmr[q];
+    }
     if (t + 1 < T) {
       const int64_t tn = t + 1;
 #pragma unroll
@@ -119,81 +112,58 @@ __global__ void __launch_bounds__(128) derive_kernel(DeriveArgs p) {
         nmr[a] = __ldg(mrv + tn * S + a);
       }
     }
-    // all-pass step, prediction.rs:73-79 (in_prev = x[t-d-1], zero while t-d-1 < 0)
-    const float2 apl01 = ap01;
-    const float apl2 = ap2;
-    if (valid) {
-      ap01 = fma2(c2, sub2(in01, ap01), inp01);
-      ap2 = fmaf(c, in2 - ap2, inp2);
+    float ap_last[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      ap_last[b] = ap[b];
+      // in_prev = x[t-d-1] (zero while t-d-1 < 0), prediction.rs:73-77
+      if (valid) ap[b] = fmaf(c, in[b] - ap[b], in_prev[b]);
+      in_prev[b] = in[b];
     }
-    inp01 = in01;
-    inp2 = in2;
-    // maximum regularisation, derivation.rs:509-535
-    const float sum = fabsf(x0) + fabsf(x1) + fabsf(x2);
+    float mreg[3];
+    const float sum = fabsf(x[0]) + fabsf(x[1]) + fabsf(x[2]);
     const bool over = sum > thr;
     const float f = sum - thr;
-    const float2 mreg01 = over ? mul2(make_float2(f, f), make_float2(copysignf(1.0f, x0), copysignf(1.0f, x1)))
-                               : make_float2(0.0f, 0.0f);
-    const float mreg2 = over ? f * copysignf(1.0f, x2) : 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) mreg[a] = over ? f * copysignf(1.0f, x[a]) : 0.0f;
     if (do_gains) {
-      // q[a] = fma(mr[a], mse/M, maxreg[a] * reg); dG[a][b] += ap[b] * q[a]
-      const float2 q01 = fma2(mr01, mse2, mul2(mreg01, reg2));
-      const float q[3] = {q01.x, q01.y, fmaf(mr2, mse_s, mreg2 * reg_s)};
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        dG01[a] = add2(dG01[a], mul2(ap01, make_float2(q[a], q[a])));
-        dG2[a] = dG2[a] + ap2 * q[a];
+        const float q = fmaf(mr[a], mse_s, mreg[a] * reg_s);
+#pragma unroll
+        for (int b = 0; b < 3; ++b) dG[a][b] = dG[a][b] + ap[b] * q;
       }
     }
     if (do_coefs) {
-      float2 e01;
-      float e2;
-      bool add = true;
       if (textbook) {
         if (t >= d) {
-          if (valid) {
-            fir01 = fma2(mc2, fir01, in01);
-            fir2 = fmaf(minus_c, fir2, in2);
-          }
-          iir01 = fma2(mc2, iir01, apl01);
-          iir2 = fmaf(minus_c, iir2, apl2);
-        }
-        e01 = sub2(fir01, iir01);
-        e2 = fir2 - iir2;
-      } else {
-        add = valid && t >= d;
-        e01 = sub2(in01, apl01);
-        e2 = in2 - apl2;
-      }
-      if (add) {
-        const float mr[3] = {mr01.x, mr01.y, mr2};
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          // ((e[b] * g[a][b]) * mr[a]) then fma(., mse/M, diff * delta^5), summed in (a, b) order
-          const float2 t01 = fma2(mul2(mul2(e01, g01[a]), make_float2(mr[a], mr[a])), mse2, drdd2);
-          const float t2 = fmaf((e2 * g2[a]) * mr[a], mse_s, dr_dd);
-          dC = dC + t01.x;
-          dC = dC + t01.y;
-          dC = dC + t2;
+          for (int b = 0; b < 3; ++b) {
+            if (valid) fir[b] = fmaf(minus_c, fir[b], in[b]);
+            iir[b] = fmaf(minus_c, iir[b], ap_last[b]);
+          }
         }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) dC = dC + fmaf((fir[b] - iir[b]) * g[a][b] * mr[a], mse_s, dr_dd);
+      } else if (valid && t >= d) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) dC = dC + fmaf((in[b] - ap_last[b]) * g[a][b] * mr[a], mse_s, dr_dd);
       }
     }
   }
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    float* dr = p.dG + (3 * v + a) * kGainCols + 3 * n;
-    dr[0] = dG01[a].x;
-    dr[1] = dG01[a].y;
-    dr[2] = dG2[a];
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) p.dG[(3 * v + a) * kGainCols + 3 * n + b] = dG[a][b];
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    p.fir[v * kGainCols + 3 * n + b] = fir[b];
+    p.iir[v * kGainCols + 3 * n + b] = iir[b];
   }
-  float* fw = p.fir + v * kGainCols + 3 * n;
-  float* iw = p.iir + v * kGainCols + 3 * n;
-  fw[0] = fir01.x;
-  fw[1] = fir01.y;
-  fw[2] = fir2;
-  iw[0] = iir01.x;
-  iw[1] = iir01.y;
-  iw[2] = iir2;
   p.dC[idx] = dC;
 }
 

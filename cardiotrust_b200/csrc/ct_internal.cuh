@@ -109,35 +109,6 @@ struct DeviceScenario {
   GridBarrier* barrier;  // [1]
 };
 
-// Packed FP32 arithmetic of sm_100 (two lanes per instruction, each rounded to nearest like the scalar
-// add.rn / sub.rn / mul.rn / fma.rn, subnormals kept): bit-identical to two scalar operations.
-__device__ __forceinline__ unsigned long long f2_bits(float2 v) {
-  return (unsigned long long)__float_as_uint(v.x) | ((unsigned long long)__float_as_uint(v.y) << 32);
-}
-__device__ __forceinline__ float2 f2_from(unsigned long long r) {
-  return make_float2(__uint_as_float((unsigned int)r), __uint_as_float((unsigned int)(r >> 32)));
-}
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {  // a * b + c, one rounding per lane
-  unsigned long long d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
-  return f2_from(d);
-}
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
-  unsigned long long d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
-  return f2_from(d);
-}
-__device__ __forceinline__ float2 add2(float2 a, float2 b) {
-  unsigned long long d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
-  return f2_from(d);
-}
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
-  unsigned long long d;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
-  return f2_from(d);
-}
-
 // Records `message` as the calling thread's last error (read by ct_last_error); returns status.
 int report_error(int status, const char* message);
 
