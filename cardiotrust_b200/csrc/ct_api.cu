@@ -576,16 +576,13 @@ void scatter_state_columns(float* dst, const float* src, const std::vector<int32
 // (voxel, offset) items read, and each item's slot in that list. False if a neighbourhood
 // exceeds kFwdHaloMax (the resident forward form is then not used).
 bool build_halos(const ct_scn* s, const std::vector<int32_t>& nbr_ref, int64_t tiles, std::vector<int32_t>& halo,
-                 std::vector<int32_t>& nhalo, std::vector<int16_t>& hslot, std::vector<int32_t>& nbt,
-                 std::vector<int32_t>& nnbt) {
-  const int TV = ct::kFwdTileVoxels, HM = ct::kFwdHaloMax, NT = ct::kFwdNbTilesMax;
+                 std::vector<int32_t>& nhalo, std::vector<int16_t>& hslot) {
+  const int TV = ct::kFwdTileVoxels, HM = ct::kFwdHaloMax;
   const int64_t V = (int64_t)s->perm.size();
   halo.assign((size_t)(tiles * HM), -1);
   nhalo.assign((size_t)tiles, 0);
   hslot.assign((size_t)(tiles * TV * kOffsets), -1);
-  nbt.assign((size_t)(tiles * NT), -1);
-  nnbt.assign((size_t)tiles, 0);
-  std::vector<int32_t> list, owners;
+  std::vector<int32_t> list;
   for (int64_t t = 0; t < tiles; ++t) {
     list.clear();
     for (int vl = 0; vl < TV; ++vl) {
@@ -601,15 +598,6 @@ bool build_halos(const ct_scn* s, const std::vector<int32_t>& nbr_ref, int64_t t
     if ((int)list.size() > HM) return false;
     nhalo[(size_t)t] = (int32_t)list.size();
     std::copy(list.begin(), list.end(), halo.begin() + (size_t)(t * HM));
-    // the other tiles whose states this tile's steps read (the tiles it waits for between blocks)
-    owners.clear();
-    for (int32_t dw : list)
-      if (dw / TV != t) owners.push_back(dw / TV);
-    std::sort(owners.begin(), owners.end());
-    owners.erase(std::unique(owners.begin(), owners.end()), owners.end());
-    if ((int)owners.size() > NT) return false;
-    nnbt[(size_t)t] = (int32_t)owners.size();
-    std::copy(owners.begin(), owners.end(), nbt.begin() + (size_t)(t * NT));
     for (int vl = 0; vl < TV; ++vl) {
       const int64_t u = t * TV + vl;
       if (u >= V) break;
@@ -900,10 +888,10 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
   // forward form: resident (one tile per CTA, halo ring) when every tile fits a co-resident CTA
   // and every tile's neighbourhood fits the ring; streaming otherwise
   const int64_t tiles = (d.V + ct::kFwdTileVoxels - 1) / ct::kFwdTileVoxels;
-  std::vector<int32_t> h_halo, h_nhalo, h_nbt, h_nnbt;
+  std::vector<int32_t> h_halo, h_nhalo;
   std::vector<int16_t> h_hslot;
   d.fwd_ring = tiles <= ct::forward_ring_capacity(ctx->device) &&
-               build_halos(s, nbr, tiles, h_halo, h_nhalo, h_hslot, h_nbt, h_nnbt);
+               build_halos(s, nbr, tiles, h_halo, h_nhalo, h_hslot);
   d.fwd_grid = d.fwd_ring ? (int)tiles : ct::forward_grid_size(d.V, ctx->device);
   {
     const int64_t tiles = ((M + 63) / 64) * ((T + 63) / 64);
@@ -980,9 +968,6 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
     ALLOC(d.halo, tiles * ct::kFwdHaloMax);
     ALLOC(d.hslot, tiles * ct::kFwdTileVoxels * kOffsets);
     ALLOC(d.nhalo, tiles);
-    ALLOC(d.nbt, tiles * ct::kFwdNbTilesMax);
-    ALLOC(d.nnbt, tiles);
-    ALLOC(d.progress, tiles);
   }
   ALLOC(d.status, 1);
   ALLOC(d.barrier, 1);
@@ -1017,8 +1002,6 @@ int ct_scenario_create(ct_ctx* ctx, const ct_scenario_desc* desc, const ct_algor
     r = r ? r : upload(s, d.halo, h_halo.data(), sizeof(int32_t) * h_halo.size());
     r = r ? r : upload(s, d.hslot, h_hslot.data(), sizeof(int16_t) * h_hslot.size());
     r = r ? r : upload(s, d.nhalo, h_nhalo.data(), sizeof(int32_t) * h_nhalo.size());
-    r = r ? r : upload(s, d.nbt, h_nbt.data(), sizeof(int32_t) * h_nbt.size());
-    r = r ? r : upload(s, d.nnbt, h_nnbt.data(), sizeof(int32_t) * h_nnbt.size());
   }
   r = r ? r : upload(s, d.u, desc->control_function, sizeof(float) * T);
   if (!r && desc->measurements) r = upload(s, d.meas, desc->measurements, sizeof(float) * B * T * M);

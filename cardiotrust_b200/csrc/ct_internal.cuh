@@ -16,7 +16,6 @@ constexpr int kGainCols = 78;  // 26 offsets x 3 neighbour components
 constexpr int kMaxStepBlock = 8;  // steps advanced between grid barriers in the forward kernel
 constexpr int kFwdTileVoxels = 32;  // voxels per forward tile (consecutive in device order)
 constexpr int kFwdHaloMax = 160;    // largest neighbourhood of a tile the resident forward form stages
-constexpr int kFwdNbTilesMax = 64;  // most tiles a resident tile's neighbourhood may touch
 constexpr int kCkptSteps = 256;     // adjoint mode: default all-pass checkpoint interval (power of two)
 
 // Device-side grid barrier state: a monotone arrival counter, zeroed before each launch.
@@ -88,9 +87,6 @@ struct DeviceScenario {
   int32_t* halo;         // [tiles, kFwdHaloMax] device voxels of each tile's neighbourhood
   int16_t* hslot;        // [tiles, 26 * kFwdTileVoxels] halo slot of each item's neighbour, -1 if absent
   int32_t* nhalo;        // [tiles]
-  int32_t* nbt;          // [tiles, kFwdNbTilesMax] other tiles holding a voxel of the tile's neighbourhood, -1 padded
-  int32_t* nnbt;         // [tiles]
-  unsigned int* progress;  // [tiles] blocks of steps each tile has completed in the running launch
   // adjoint mode (ct_adjoint.cu), allocated on first use
   int32_t* rev;          // [V,26] voxel whose offset n points at this voxel, -1 if none
   int ckpt_k;            // checkpoint interval K (power of two)

@@ -56,47 +56,6 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* bar, unsigned int numb
   return s_ok != 0;
 }
 
-__device__ __forceinline__ void st_release_gpu(unsigned int* p, unsigned int v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Neighbour-only barrier of a cooperative launch in which CTA `me` owns one tile: publishes that the
-// CTA has completed `done` blocks of steps (progress[me] = done, release) and waits until each of
-// the `count` tiles in `others` has completed at least `done` blocks (acquire). The CTA barrier on
-// entry orders every thread's writes of the block before the release; the one on exit orders the
-// waiting lanes' acquires before every thread's later reads. One lane of warp 0 polls per listed
-// tile; each poll is bounded (~2 s of globaltimer): on expiry the CTA records CT_ERR_TIMEOUT in
-// *status and returns false, and CTAs also leave once another CTA has recorded an error.
-__device__ __forceinline__ bool tile_wait(unsigned int* progress, int me, unsigned int done, const int32_t* others,
-                                          int count, int32_t* status) {
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    if (threadIdx.x == 0) st_release_gpu(&progress[me], done);
-    int ok = 1;
-    for (int i = (int)threadIdx.x; i < count && ok; i += 32) {
-      const unsigned int* flag = &progress[others[i]];
-      if (ld_acquire_gpu(flag) >= done) continue;
-      const unsigned long long t0 = global_ns();
-      while (ld_acquire_gpu(flag) < done) {
-        if (*(volatile int32_t*)status != 0) {
-          ok = 0;
-          break;
-        }
-        if (global_ns() - t0 > 2000000000ull) {
-          atomicCAS(status, 0, (int32_t)CT_ERR_TIMEOUT);
-          ok = 0;
-          break;
-        }
-      }
-    }
-    ok = __all_sync(0xffffffffu, ok);
-    if (threadIdx.x == 0) s_ok = ok;
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
-
 // Cooperative launch (all CTAs co-resident, required by grid_barrier) through cudaLaunchKernelExC with
 // the cooperative attribute, which stream capture records as a cooperative kernel node.
 inline cudaError_t launch_cooperative(const void* func, int grid, int block, void** args, size_t smem,
