@@ -46,8 +46,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default=WORKLOAD)
-    p.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "tf32", "bf16x6"],
-                   help="measurement products: FP32 CUDA cores, tcgen05 split TF32, tcgen05 TF32")
+    p.add_argument("--precision", default="bf16x6", choices=["fp32", "tf32x3", "tf32", "bf16x6"],
+                   help="measurement products: FP32 CUDA cores, tcgen05 3xTF32 / TF32 (guarded), tcgen05 BF16 on "
+                        "error-free slices (exact accumulation)")
     p.add_argument("--batch-scenarios", type=int, default=64,
                    help="scenarios of the batched section (0 skips it)")
     p.add_argument("--batch-epochs", type=int, default=3, help="timed epochs of the batched section")
