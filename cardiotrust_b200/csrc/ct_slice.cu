@@ -140,12 +140,12 @@ __global__ void reduce_parts_kernel(const float* __restrict__ part, int ksplit, 
 
 // ---- the sliced GEMM
 
-template <int NT>
+template <int NT, int STAGES>
 struct SliceSmem {
   static constexpr int kA = kRows * kChunk * 2;  // one slice of an A tile: 16 KB
   static constexpr int kB = NT * kChunk * 2;     // one slice of a B tile
   static constexpr int kStage = kSlices * (kA + kB);
-  static constexpr int kStages = NT <= 64 ? 3 : 2;
+  static constexpr int kStages = STAGES;
   static constexpr int kBytes = kStages * kStage + 1024 /* alignment */ + 256 /* barriers */;
 };
 
@@ -162,13 +162,15 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 // C[z][m0 + r][n0 + c] = sum over the CTA's groups of the sliced product of A[m0 + r, :] and
 // B[n0 + c, :]. map_a / map_b: 3D maps {K, rows, 3 slices} of BF16, box {64, 128 | NT, 3}.
 // sa [rows][ng] and sb [ng][cols]: the scales. chunks_per_split is a multiple of kGroupChunks.
-template <int NT>
+// STAGES: shared-memory stages of the TMA ring (2 for long K; 1 for the short K of H^T r, where two
+// CTAs share an SM and one's epilogue overlaps the other's loads and MMAs).
+template <int NT, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1)
     slice_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                       const float* __restrict__ sa, const float* __restrict__ sb, int ng, float* __restrict__ C,
                       int ldc, long long c_split_stride, int rows, int cols, int kchunks, int chunks_per_split,
                       int32_t* status) {
-  using L = SliceSmem<NT>;
+  using L = SliceSmem<NT, STAGES>;
   constexpr int kStages = L::kStages;
   constexpr int kTmemCols = 4 * NT;  // acc0, acc1, acc2, promoted sum
   static_assert(kTmemCols == 256 || kTmemCols == 512, "tensor-memory allocation must be a power of two");
@@ -355,23 +357,33 @@ bool make_slice_map(CUtensorMap* map, const __nv_bfloat16* ptr, int64_t inner, i
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int NT>
+// Dynamic shared memory of a launch: the layout's bytes, raised so that at most kCtasPerSm CTAs share
+// an SM (their tensor memory, 4 NT columns each, must fit the SM's 512 together).
+template <int NT, int STAGES>
+constexpr int slice_smem_bytes() {
+  constexpr int kCtasPerSm = 512 / (4 * NT);
+  constexpr int kFloor = (232448 / (kCtasPerSm + 1)) + 1024;
+  return SliceSmem<NT, STAGES>::kBytes > kFloor ? SliceSmem<NT, STAGES>::kBytes : kFloor;
+}
+
+template <int NT, int STAGES>
 cudaError_t launch_slice_gemm(const CUtensorMap& a, const CUtensorMap& b, const float* sa, const float* sb, int ng,
                               float* C, int ldc, long long split_stride, int rows, int cols, int kchunks, int per,
                               int ksplit, int32_t* status, cudaStream_t stream) {
-  using L = SliceSmem<NT>;
+  constexpr int kSmem = slice_smem_bytes<NT, STAGES>();
+  static_assert(kSmem <= 232448, "shared memory per CTA");
   static bool configured[128] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 128 && !configured[dev]) {
     cudaError_t e =
-        cudaFuncSetAttribute(slice_gemm_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kBytes);
+        cudaFuncSetAttribute(slice_gemm_kernel<NT, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
     if (e != cudaSuccess) return e;
     configured[dev] = true;
   }
   dim3 grid((unsigned)((cols + NT - 1) / NT), (unsigned)((rows + kRows - 1) / kRows), (unsigned)ksplit);
-  slice_gemm_kernel<NT><<<grid, kThreads, L::kBytes, stream>>>(a, b, sa, sb, ng, C, ldc, split_stride, rows, cols,
-                                                               kchunks, per, status);
+  slice_gemm_kernel<NT, STAGES><<<grid, kThreads, kSmem, stream>>>(a, b, sa, sb, ng, C, ldc, split_stride, rows,
+                                                                   cols, kchunks, per, status);
   return cudaGetLastError();
 }
 
@@ -443,7 +455,7 @@ cudaError_t launch_measure_sliced(DeviceScenario& d, int64_t beat, bool with_res
   const int ks = (groups + per_groups - 1) / per_groups;
   const int per = per_groups * kGroupChunks;
   const int ldp = (int)(((M + 127) / 128) * 128);
-  e = launch_slice_gemm<128>(ma, mb, d.X_sc, d.H_sc + beat * M * ngs, (int)ngs, d.gemm_part, ldp,
+  e = launch_slice_gemm<128, 2>(ma, mb, d.X_sc, d.H_sc + beat * M * ngs, (int)ngs, d.gemm_part, ldp,
                              (long long)T * ldp, (int)T, (int)M, kchunks, per, ks, d.status, stream);
   if (e != cudaSuccess) return e;
   const int64_t n = T * M;
@@ -462,10 +474,10 @@ cudaError_t launch_map_residuals_sliced(DeviceScenario& d, int64_t beat, cudaStr
   if (e != cudaSuccess) return e;
   CUtensorMap ma, mb;
   if (!make_slice_map(&ma, d.R_sl, kpm, T, kRows) ||
-      !make_slice_map(&mb, d.Ht_sl + beat * kSlices * S * kpm, kpm, S, 128))
+      !make_slice_map(&mb, d.Ht_sl + beat * kSlices * S * kpm, kpm, S, 64))
     return cudaErrorInvalidValue;
   const int kchunks = (int)(kpm / kChunk);
-  return launch_slice_gemm<128>(ma, mb, d.R_sc, d.Ht_sc + beat * S * ngm, (int)ngm, d.MR, (int)S, 0, (int)T, (int)S,
+  return launch_slice_gemm<64, 1>(ma, mb, d.R_sc, d.Ht_sc + beat * S * ngm, (int)ngm, d.MR, (int)S, 0, (int)T, (int)S,
                                 kchunks, (int)(ngm * kGroupChunks), 1, d.status, stream);
 }
 
