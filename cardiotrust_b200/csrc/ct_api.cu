@@ -408,7 +408,7 @@ int run_beat(ct_scn* s, int64_t beat, int precision, int grad_mode) {
     ds.ap_derivative = a.ap_derivative;
     CT_CUDA(run_phase(s, CT_PHASE_DERIVE, 1, [&] { return ct::launch_derive(d, ds, st); }), "derivation kernel");
   }
-  CT_CUDA(run_phase(s, CT_PHASE_STEP_METRICS, 1,
+  CT_CUDA(run_phase(s, CT_PHASE_STEP_METRICS, 2,
                     [&] { return ct::launch_step_metrics(d, a.maximum_regularization_strength, st); }),
           "step metrics kernel");
   return CT_OK;

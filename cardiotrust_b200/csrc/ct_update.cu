@@ -140,10 +140,26 @@ __global__ void smoothness_kernel(const float* __restrict__ avg, const int32_t* 
 
 // ---- metrics::calculate_step (metrics.rs:180-196) for all steps of a beat.
 // stepsum[t] = sum over forward CTAs of their partial max-regularisation sums
-// (fixed order), then a deterministic block scan gives the running sum.
-__global__ void step_metrics_kernel(const float* __restrict__ part, int grid, int64_t T, float reg,
+// (step_sum_kernel: one warp per step, a fixed order), then a deterministic block
+// scan gives the running sum.
+
+// out[t] = sum over c of part[t * grid + c]: lane l adds the partials l, l + 32, ... in order, then a
+// fixed butterfly combines the lanes, so every run and every caller gets the same sum.
+__global__ void step_sum_kernel(const float* __restrict__ part, int grid, int64_t T, float* __restrict__ out) {
+  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= T) return;
+  float s = 0.0f;
+  for (int c = lane; c < grid; c += 32) s = s + part[t * grid + c];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) out[t] = s;
+}
+
+// `part` may alias `loss_mr`: each step's value is read before the same thread writes it.
+__global__ void step_metrics_kernel(const float* part, int grid, int64_t T, float reg,
                                     float* __restrict__ mreg_sum, const float* __restrict__ loss_mse,
-                                    float* __restrict__ loss_mr, float* __restrict__ loss) {
+                                    float* loss_mr, float* __restrict__ loss) {
   constexpr int kT = 1024;
   __shared__ float warp_tot[kT / 32];
   __shared__ float carry_s;
@@ -306,10 +322,10 @@ cudaError_t launch_smoothness(DeviceScenario& d, float strength, cudaStream_t st
   return cudaGetLastError();
 }
 
+// The per-step sums go to loss_mr, which the scan then overwrites with the running sum in place (each
+// step's value is read and written by the same thread).
 cudaError_t launch_step_metrics(DeviceScenario& d, float reg_strength, cudaStream_t stream) {
-  step_metrics_kernel<<<1, 1024, 0, stream>>>(d.stepsum_part, d.fwd_grid, d.T, reg_strength, d.mreg_sum, d.loss_mse,
-                                              d.loss_mr, d.loss);
-  return cudaGetLastError();
+  return launch_step_metrics_parts(d, d.stepsum_part, d.fwd_grid, reg_strength, stream);
 }
 
 cudaError_t launch_batch_metrics(DeviceScenario& d, int64_t index, cudaStream_t stream) {
@@ -326,7 +342,11 @@ cudaError_t launch_batch_metrics_dev(DeviceScenario& d, const int64_t* index_dev
 
 cudaError_t launch_step_metrics_parts(DeviceScenario& d, const float* part, int parts, float reg_strength,
                                       cudaStream_t stream) {
-  step_metrics_kernel<<<1, 1024, 0, stream>>>(part, parts, d.T, reg_strength, d.mreg_sum, d.loss_mse, d.loss_mr,
+  const int64_t threads = d.T * 32;
+  step_sum_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(part, parts, d.T, d.loss_mr);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  step_metrics_kernel<<<1, 1024, 0, stream>>>(d.loss_mr, 1, d.T, reg_strength, d.mreg_sum, d.loss_mse, d.loss_mr,
                                               d.loss);
   return cudaGetLastError();
 }
