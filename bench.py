@@ -575,6 +575,23 @@ def precision_reference(workload, steps):
     adj.stated_loss(a, gradient=True)
     out["adjoint_grad_gains"] = adj.d_gains.copy()
     out["adjoint_grad_coefs"] = adj.d_coefs.copy()
+    del adj
+    # the reference's own arithmetic: the f32 restatement (reference loop order) against the same f64
+    def rel(x, y):
+        y = np.asarray(y, np.float64)
+        return float(np.linalg.norm(np.asarray(x, np.float64) - y) / max(np.linalg.norm(y), 1e-300))
+
+    f32 = oracle.from_scenario(scn)
+    f32.run_epoch(a)
+    f32_err = {k: rel(v, out[k]) for k, v in (("system_states", f32.system_states), ("measurements", f32.measurements),
+                                               ("residuals", f32.residuals), ("grad_gains", f32.d_gains),
+                                               ("grad_coefs", f32.d_coefs))}
+    del f32
+    f32 = oracle.from_scenario(scn)
+    f32.run_epoch(a, adjoint=True)
+    f32_err["adjoint_grad_gains"] = rel(f32.d_gains, out["adjoint_grad_gains"])
+    f32_err["adjoint_grad_coefs"] = rel(f32.d_coefs, out["adjoint_grad_coefs"])
+    out["f32_reference"] = f32_err
     return scn, out
 
 
@@ -629,6 +646,7 @@ def precision_case(alg, ctx, scn, ref):
         r["adjoint_grad_coefs"] = rel(eng.read("grad_coefs"), ref["adjoint_grad_coefs"])
         eng.close()
         results[name] = r
+    results["f32_reference_restatement (CPU, reference loop order)"] = ref["f32_reference"]
     return {
         "workload": f"{scn.spec.mask} {scn.spec.shape} ({scn.num_voxels} voxels, {scn.num_states} states), "
                     f"{scn.num_sensors} sensor rows, beat cut to {scn.num_steps} steps so the f64 CPU oracle "
