@@ -51,18 +51,20 @@ def _engines(alg, ctx, members, algo):
     return [alg.EpochEngine.from_scenario(ctx, m, num_batch_slots=8, algorithm=algo) for m in members]
 
 
+@pytest.mark.parametrize("precision", ["Fp32", "Bf16x6"])
 @pytest.mark.parametrize("mode", ["reference", "adjoint"])
-def test_batch_matches_single_runs(alg, ctx, members, mode):
+def test_batch_matches_single_runs(alg, ctx, members, mode, precision):
     gm = alg.GradMode.Adjoint if mode == "adjoint" else alg.GradMode.Reference
+    prec = alg.Precision[precision]
     algo = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-3, freeze_delays=False)
     batched = _engines(alg, ctx, members, algo)
     single = _engines(alg, ctx, members, algo)
-    batch = alg.EpochBatch(ctx, batched, grad_mode=gm, precision=alg.Precision.Fp32)
+    batch = alg.EpochBatch(ctx, batched, grad_mode=gm, precision=prec)
     for epoch in range(2):
         idx = batch.run_epoch()
         assert list(idx) == [epoch + 1] * len(members)
         for m, e in zip(members, single):
-            e.run_epoch(epoch, beat_order=np.arange(m.num_beats), grad_mode=gm)
+            e.run_epoch(epoch, beat_order=np.arange(m.num_beats), grad_mode=gm, precision=prec)
         for k, (b, e) in enumerate(zip(batched, single)):
             if epoch == 0:
                 np.testing.assert_array_equal(b.read("system_states"), e.read("system_states"), err_msg=str(k))
