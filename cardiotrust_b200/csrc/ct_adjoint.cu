@@ -55,7 +55,7 @@ constexpr int kAdjThreads = 512;
 constexpr int kGroup = 16;                 // threads per voxel (a half warp)
 constexpr int kCols = 5;                   // columns per thread: k = lane + 16 i, k < 78
 constexpr int kWarps = kAdjThreads / 32;
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every mbarrier wait
 static_assert(kTileVoxels * kGroup == kAdjThreads, "one voxel group per 16 threads");
 static_assert(kCols * kGroup >= kGainCols, "columns per voxel");
@@ -181,7 +181,7 @@ __device__ __forceinline__ void recompute_segment(const AdjScn& p, int v0, int n
       }
     }
   }
-  constexpr int kU = 2;
+  constexpr int kU = 4;
   for (int t0 = t_lo; t0 < t_hi; t0 += kU) {
     float in[kU][kCols];
 #pragma unroll

@@ -748,7 +748,7 @@ __global__ void __launch_bounds__(kThreads, 2) forward_ring_kernel(FwdArgs p, Ri
           if (vl < nv) {
             const float* aps = sm.ap_out[buf][s2] + vl * kGainCols;
             float x0 = 0.0f, x1 = 0.0f, x2 = 0.0f;
-#pragma unroll 3
+#pragma unroll
             for (int k = 0; k < kGainCols; k += 2) {
               const float2 a = *reinterpret_cast<const float2*>(aps + k);
               const float4 g0 = sm.g[k][vl];
