@@ -59,6 +59,7 @@ constexpr int kStages = 3;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every mbarrier wait
 static_assert(kTileVoxels * kGroup == kAdjThreads, "one voxel group per 16 threads");
 static_assert(kCols * kGroup >= kGainCols, "columns per voxel");
+static_assert(kGroup == 16 && kCols == 5 && 4 * kGroup < kGainCols, "the inbox sum's column grouping");
 
 struct AdjSmem {
   float g[kTileVoxels * 3 * kGainCols];  // the tile's gain rows, [voxel][row a][column k] as in HBM
@@ -213,7 +214,7 @@ __device__ __forceinline__ void recompute_segment(const AdjScn& p, int v0, int n
 struct Cols {
   float c[kCols], lprev[kCols], dg[kCols][3], dc[kCols];
   int d[kCols], jw[kCols];  // delay; inbox cell neighbour * 78 + column, -1 if unconnected
-  int xo[kCols];            // state index 3 * neighbour + b of the column's input
+  int xo[kCols];            // offset of the column's input x[t-d-1, 3 * neighbour + b] from row t: state - (d+1) S
   uint32_t full_ph;         // bit s: parity of the next completion of full[s]
   uint32_t empty_ph;        // thread 0: parity of the next completion of empty[s]
   uint32_t empty_wait;      // thread 0: bit s: a use of stage s has not been waited empty yet
@@ -256,7 +257,9 @@ __device__ __forceinline__ bool load_cols(Cols& cs, AdjSmem& sm, const AdjScn& p
         cs.c[i] = sm.coef[it];
         cs.d[i] = sm.del[it];
         cs.jw[i] = nb * kGainCols + k;
-        cs.xo[i] = 3 * nb + k % 3;
+        // fits 32 bits: (d + 1) S < 2^31 whenever the inbox ring of at least d + 9 planes of 26 S
+        // floats fits in device memory
+        cs.xo[i] = 3 * nb + k % 3 - (cs.d[i] + 1) * p.S;
       }
       if (state) cs.lprev[i] = sm.lam[vl * kGainCols + k];
     }
@@ -321,11 +324,12 @@ __device__ __forceinline__ void issue_xm(const Cols& cs, AdjSmem& sm, const AdjS
       const size_t off = (size_t)t * p.S + 3 * (v0 + vl) + (q % 3);
       cp_async4(&sm.xm[st][vl][q], (q < 3 ? p.X : p.MR) + off);
     }
+    const float* xrow = p.X + (size_t)t * p.S;
 #pragma unroll
     for (int i = 0; i < kCols; ++i) {
       const int t1 = t - cs.d[i] - 1;
       if (cs.jw[i] >= 0 && t1 >= 0)
-        cp_async4(&sm.stage[st][2][vl * kGainCols + my_col(i)], p.X + (size_t)t1 * p.S + cs.xo[i]);
+        cp_async4(&sm.stage[st][2][vl * kGainCols + my_col(i)], xrow + cs.xo[i]);
     }
   }
   cp_async_commit();
@@ -362,18 +366,21 @@ __device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem& sm, const AdjS
     __syncwarp();                  // the voxel group's copies of step t
     // lx[t] of the voxel: instantaneous terms + its 78 inbox cells (partial sums per component,
     // reduced over the 16-thread group in a fixed order)
-    float pb[3] = {0.0f, 0.0f, 0.0f};
+    // column k = q + 16 i has component b = (q + i) mod 3 (16 = 1 mod 3): sum the columns i = j,
+    // j + 3 (in order) into r[j], then rotate by q mod 3 so that pb[b] holds component b
     const float* in_row = sm.stage[st][0] + vl * kGainCols;
+    const int q16 = threadIdx.x % kGroup;
+    float r[3];
+    r[0] = in_row[q16] + in_row[q16 + 3 * kGroup];
+    r[1] = in_row[q16 + kGroup] + (q16 + 4 * kGroup < kGainCols ? in_row[q16 + 4 * kGroup] : 0.0f);
+    r[2] = in_row[q16 + 2 * kGroup];
+    const int rot = q16 % 3;
+    float pb[3];
 #pragma unroll
-    for (int i = 0; i < kCols; ++i) {
-      const int k = my_col(i);
-      if (k < kGainCols) {
-        const float v = in_row[k];
-        const int b = k % 3;
-        pb[0] = pb[0] + (b == 0 ? v : 0.0f);
-        pb[1] = pb[1] + (b == 1 ? v : 0.0f);
-        pb[2] = pb[2] + (b == 2 ? v : 0.0f);
-      }
+    for (int b = 0; b < 3; ++b) {
+      // pb[b] = r[(b - rot) mod 3]
+      const int j = b - rot;
+      pb[b] = j == 0 ? r[0] : ((j == 1 || j == -2) ? r[1] : r[2]);
     }
 #pragma unroll
     for (int off = kGroup / 2; off > 0; off >>= 1)
