@@ -32,7 +32,7 @@
 //   * Pipeline. Sixteen threads (half a warp) own one voxel of the tile, five
 //     of its 78 columns each. A step's inbox row and q row (contiguous per
 //     tile; plane pitch padded to 16 bytes) arrive by TMA bulk copies into a
-//     ring of kStages shared-memory stages, issued kStages steps ahead by one
+//     ring of NS shared-memory stages (3, or 4 for a batch), issued NS steps ahead by one
 //     thread and completed on a `full` mbarrier per stage; the states, mapped
 //     residuals and in1 gathers of the step arrive by cp.async. Warps run
 //     decoupled: each releases a stage on an `empty` mbarrier, and no CTA
@@ -55,22 +55,27 @@ constexpr int kAdjThreads = 512;
 constexpr int kGroup = 16;                 // threads per voxel (a half warp)
 constexpr int kCols = 5;                   // columns per thread: k = lane + 16 i, k < 78
 constexpr int kWarps = kAdjThreads / 32;
-constexpr int kStages = 3;
+// Stages of the copy ring: 3 for one scenario's tiles (more L1 left for the gathers: cuboid20
+// adjoint 11.8 ms against 12.4 ms with 4), 4 for a batch's tile list (each CTA walks many tiles,
+// whose pipelines start cold: 64-scenario batched adjoint 3.40 s against 3.50 s with 3).
+constexpr int kStagesSingle = 3;
+constexpr int kStagesBatch = 4;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every mbarrier wait
 static_assert(kTileVoxels * kGroup == kAdjThreads, "one voxel group per 16 threads");
 static_assert(kCols * kGroup >= kGainCols, "columns per voxel");
 static_assert(kGroup == 16 && kCols == 5 && 4 * kGroup < kGainCols, "the inbox sum's column grouping");
 
+template <int NS>
 struct AdjSmem {
   float g[kTileVoxels * 3 * kGainCols];  // the tile's gain rows, [voxel][row a][column k] as in HBM
-  float stage[kStages][3][kTileCols];    // [stage][inbox | q | in1][voxel * 78 + column]
-  float xm[kStages][kTileVoxels][8];     // [stage][voxel][x0 x1 x2 mr0 mr1 mr2 - -]
+  float stage[NS][3][kTileCols];    // [stage][inbox | q | in1][voxel * 78 + column]
+  float xm[NS][kTileVoxels][8];     // [stage][voxel][x0 x1 x2 mr0 mr1 mr2 - -]
   float coef[kTileItems];                // per (voxel, offset) of the tile
   int32_t del[kTileItems];
   int32_t nbr[kTileItems];
   float lam[kTileCols];                  // adjoint state carried between blocks (tiles that are not resident)
-  uint64_t full[kStages];                // the stage's rows have landed
-  uint64_t empty[kStages];               // every warp is done with the stage
+  uint64_t full[NS];                // the stage's rows have landed
+  uint64_t empty[NS];               // every warp is done with the stage
   uint64_t meta_bar;
   int abort;
   AdjScn sp;                             // scenario of the current tile
@@ -145,7 +150,8 @@ __device__ __forceinline__ void tile_of(const AdjLaunch& L, int tile, int* scn, 
   }
 }
 
-__device__ __forceinline__ void load_scn(AdjSmem& sm, const AdjLaunch& L, int scn) {
+template <int NS>
+__device__ __forceinline__ void load_scn(AdjSmem<NS>& sm, const AdjLaunch& L, int scn) {
   __syncthreads();
   if (threadIdx.x == 0) sm.sp = L.scns ? L.scns[scn] : L.single;
   __syncthreads();
@@ -225,7 +231,8 @@ struct Cols {
 // Per-tile tables into shared memory by bulk copies (gains, coefficients, delays, neighbours and,
 // with `state`, the adjoint state of the previous block), then each thread's column registers.
 // Called by all threads after a CTA barrier.
-__device__ __forceinline__ bool load_cols(Cols& cs, AdjSmem& sm, const AdjScn& p, int v0, int nv, bool state,
+template <int NS>
+__device__ __forceinline__ bool load_cols(Cols& cs, AdjSmem<NS>& sm, const AdjScn& p, int v0, int nv, bool state,
                                           int32_t* status) {
   if (threadIdx.x == 0) {
     const uint32_t gb = (uint32_t)((nv * 3 * kGainCols * 4 + 15) & ~15);
@@ -294,7 +301,8 @@ __device__ __forceinline__ void flush_cols(Cols& cs, const AdjScn& p, int v0, in
 
 // Thread 0: bulk copies of step t's inbox and q rows of the tile into stage `st`, once every
 // warp has released the stage's previous use.
-__device__ __forceinline__ bool issue_stage(Cols& cs, AdjSmem& sm, const AdjScn& p, int st, int v0, int nv, int t,
+template <int NS>
+__device__ __forceinline__ bool issue_stage(Cols& cs, AdjSmem<NS>& sm, const AdjScn& p, int st, int v0, int nv, int t,
                                            int t_lo, int32_t* status) {
   if (cs.empty_wait & (1u << st)) {
     if (!mbar_wait(&sm.empty[st], (cs.empty_ph >> st) & 1u, status)) return false;
@@ -316,7 +324,8 @@ __device__ __forceinline__ bool issue_stage(Cols& cs, AdjSmem& sm, const AdjScn&
 // Per thread, into stage `st` for step t: threads 0-5 of each voxel group copy the voxel's states
 // and mapped residuals; every thread gathers in1_t = x[t-d-1, j] of its connected columns. One
 // cp.async group per stage and thread, committed even when empty.
-__device__ __forceinline__ void issue_xm(const Cols& cs, AdjSmem& sm, const AdjScn& p, int st, int v0, int nv, int t,
+template <int NS>
+__device__ __forceinline__ void issue_xm(const Cols& cs, AdjSmem<NS>& sm, const AdjScn& p, int st, int v0, int nv, int t,
                                          bool real) {
   const int vl = my_voxel(), q = threadIdx.x % kGroup;
   if (real && vl < nv) {
@@ -338,7 +347,8 @@ __device__ __forceinline__ void issue_xm(const Cols& cs, AdjSmem& sm, const AdjS
 // Steps ta down to t_end (inclusive) of one tile; t_lo is the segment's first step (row 0 of seg_q).
 // Warps run decoupled: a step's rows arrive on full[st], each warp releases them on empty[st].
 // Returns false if a wait timed out (the CTA must leave).
-__device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem& sm, const AdjScn& p, int v0, int nv, int ta,
+template <int NS>
+__device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem<NS>& sm, const AdjScn& p, int v0, int nv, int ta,
                                                int t_end, int t_lo, int32_t* status) {
   const size_t pitch = (size_t)p.pitch;
   const int rmask = p.ring - 1;
@@ -349,12 +359,12 @@ __device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem& sm, const AdjS
   // blocks, made visible by the grid barrier) before the async-proxy reads, in issue_stage
   if (threadIdx.x == 0) {
     asm volatile("fence.proxy.async;" ::: "memory");
-    for (int s = 0; s < kStages && ta - s >= t_end; ++s)
+    for (int s = 0; s < NS && ta - s >= t_end; ++s)
       if (!issue_stage(cs, sm, p, s, v0, nv, ta - s, t_lo, status)) sm.abort = 1;
   }
-  for (int s = 0; s < kStages; ++s) issue_xm(cs, sm, p, s, v0, nv, ta - s, ta - s >= t_end);
+  for (int s = 0; s < NS; ++s) issue_xm(cs, sm, p, s, v0, nv, ta - s, ta - s >= t_end);
   for (int t = ta; t >= t_end; --t) {
-    const int st = (ta - t) % kStages;
+    const int st = (ta - t) % NS;
     if (*(volatile int*)&sm.abort) return false;
     if (!mbar_wait(&sm.full[st], (cs.full_ph >> st) & 1u, status)) {
       sm.abort = 1;
@@ -362,7 +372,7 @@ __device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem& sm, const AdjS
     }
     cs.full_ph ^= 1u << st;
     cs.inflight &= ~(1u << st);
-    cp_async_wait<kStages - 1>();  // this thread's copies of step t
+    cp_async_wait<NS - 1>();  // this thread's copies of step t
     __syncwarp();                  // the voxel group's copies of step t
     // lx[t] of the voxel: instantaneous terms + its 78 inbox cells (partial sums per component,
     // reduced over the 16-thread group in a fixed order)
@@ -421,23 +431,25 @@ __device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem& sm, const AdjS
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty[st]);
-    issue_xm(cs, sm, p, st, v0, nv, t - kStages, t - kStages >= t_end);
-    if (threadIdx.x == 0 && t - kStages >= t_end)
-      if (!issue_stage(cs, sm, p, st, v0, nv, t - kStages, t_lo, status)) sm.abort = 1;
+    issue_xm(cs, sm, p, st, v0, nv, t - NS, t - NS >= t_end);
+    if (threadIdx.x == 0 && t - NS >= t_end)
+      if (!issue_stage(cs, sm, p, st, v0, nv, t - NS, t_lo, status)) sm.abort = 1;
   }
   return true;
 }
 
 // After a timed-out wait: let every bulk copy still in flight land (bounded) before the CTA leaves.
-__device__ __forceinline__ void drain_stages(Cols& cs, AdjSmem& sm, int32_t* status) {
+template <int NS>
+__device__ __forceinline__ void drain_stages(Cols& cs, AdjSmem<NS>& sm, int32_t* status) {
   if (threadIdx.x == 0)
-    for (int st = 0; st < kStages; ++st)
+    for (int st = 0; st < NS; ++st)
       if (cs.inflight & (1u << st)) mbar_wait(&sm.full[st], (cs.full_ph >> st) & 1u, status);
 }
 
+template <int NS>
 __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjLaunch L) {  // <= 128 registers
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  AdjSmem& sm = *reinterpret_cast<AdjSmem*>(smem_raw);
+  AdjSmem<NS>& sm = *reinterpret_cast<AdjSmem<NS>*>(smem_raw);
   const int ntiles = L.ntiles;
   const bool resident = ntiles <= (int)gridDim.x;
   // steps per block: the smallest delay of any scenario (capped); every inbox must span the delays
@@ -457,7 +469,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjLaunch L) { 
     return;
   }
   if (threadIdx.x == 0) {
-    for (int st = 0; st < kStages; ++st) {
+    for (int st = 0; st < NS; ++st) {
       mbar_init(&sm.full[st], 1);
       mbar_init(&sm.empty[st], kWarps);
     }
@@ -558,8 +570,10 @@ bool configure(int device) {
   static bool done[128] = {};
   if (device < 0 || device >= 128) return false;
   if (!done[device]) {
-    if (cudaFuncSetAttribute(adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdjSmem)) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(adjoint_kernel<kStagesSingle>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(AdjSmem<kStagesSingle>)) != cudaSuccess ||
+        cudaFuncSetAttribute(adjoint_kernel<kStagesBatch>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(AdjSmem<kStagesBatch>)) != cudaSuccess)
       return false;
     done[device] = true;
   }
@@ -572,7 +586,9 @@ int adjoint_capacity(int device) {
   configure(device);
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, kAdjThreads, sizeof(AdjSmem));
+  // both forms fit one CTA per SM (kAdjThreads threads of at most 128 registers)
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel<kStagesBatch>, kAdjThreads,
+                                                sizeof(AdjSmem<kStagesBatch>));
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
 }
@@ -618,7 +634,11 @@ cudaError_t launch_adjoint_tiles(const AdjLaunch& launch, int grid, cudaStream_t
   if (err != cudaSuccess) return err;
   AdjLaunch l = launch;
   void* args[] = {&l};
-  return launch_cooperative((const void*)adjoint_kernel, grid, kAdjThreads, args, sizeof(AdjSmem), stream);
+  if (l.tiles)  // a batch's tile list
+    return launch_cooperative((const void*)adjoint_kernel<kStagesBatch>, grid, kAdjThreads, args,
+                              sizeof(AdjSmem<kStagesBatch>), stream);
+  return launch_cooperative((const void*)adjoint_kernel<kStagesSingle>, grid, kAdjThreads, args,
+                            sizeof(AdjSmem<kStagesSingle>), stream);
 }
 
 cudaError_t launch_adjoint(DeviceScenario& d, const AdjointScalars& s, cudaStream_t stream) {
