@@ -52,6 +52,7 @@ namespace ct {
 namespace {
 
 constexpr int kTileVoxels = kFwdTileVoxels;
+constexpr int kFwdScnCache = 64;  // scenarios of a batched launch kept in shared memory
 constexpr int kTileStates = 3 * kTileVoxels;
 constexpr int kTileItems = kTileVoxels * kOffsets;  // (voxel, offset) pairs
 constexpr int kRound = 2;                            // steps per round
@@ -419,7 +420,12 @@ __global__ void __launch_bounds__(kThreads, 2) forward_stream_kernel(FwdArgs p) 
 __global__ void __launch_bounds__(kThreads, 2) forward_batch_kernel(FwdBatch B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
-  __shared__ FwdArgs sp;
+  // the launch's first kFwdScnCache scenarios, copied into shared memory once; a tile of any other
+  // scenario loads it into `over` at the start of its visit
+  __shared__ FwdArgs cache[kFwdScnCache];
+  __shared__ FwdArgs over;
+  for (int i = threadIdx.x; i < min(B.nscn, kFwdScnCache); i += blockDim.x) cache[i] = B.scns[i];
+  auto scn_of = [&](int s) -> const FwdArgs& { return s < kFwdScnCache ? cache[s] : B.scns[s]; };
   int Lmax = kMaxStepBlock;
   for (int s = 0; s < B.nscn; ++s) {
     int dmin = B.scns[s].dmin[0];
@@ -431,23 +437,25 @@ __global__ void __launch_bounds__(kThreads, 2) forward_batch_kernel(FwdBatch B) 
   // the CTA's first tile at or after list index `from` whose scenario still runs at step t0
   auto next_live = [&](int from, int t0) {
     int tile = from;
-    while (tile < B.ntiles && t0 >= B.scns[B.tiles[tile].x].T) tile += gridDim.x;
+    while (tile < B.ntiles && t0 >= scn_of(B.tiles[tile].x).T) tile += gridDim.x;
     return tile;
   };
+  __syncthreads();
   unsigned int barrier_number = 0;
   for (int t0 = 0; t0 < B.Tmax; t0 += Lmax) {
     int tile = next_live(blockIdx.x, t0);
     __syncthreads();
     if (tile < B.ntiles) {
       const int2 tl = B.tiles[tile];
-      stage_load(nx, B.scns[tl.x], tl.y);
+      stage_load(nx, scn_of(tl.x), tl.y);
       stage_store(sm, nx);
     }
     while (tile < B.ntiles) {
       const int2 tl = B.tiles[tile];
-      if (threadIdx.x == 0) sp = B.scns[tl.x];
+      if (threadIdx.x == 0 && tl.x >= kFwdScnCache) over = B.scns[tl.x];
       if (threadIdx.x < kMaxStepBlock) sm.part[threadIdx.x] = 0.0f;
       __syncthreads();
+      const FwdArgs& sp = tl.x < kFwdScnCache ? cache[tl.x] : over;
       const int L = (sp.T - t0) < Lmax ? (sp.T - t0) : Lmax;
       const int v0 = tl.y;
       const int nv = min(kTileVoxels, sp.V - v0);
@@ -456,7 +464,7 @@ __global__ void __launch_bounds__(kThreads, 2) forward_batch_kernel(FwdBatch B) 
       const int2 ntl = more ? B.tiles[nt] : make_int2(0, 0);
       const int dmax = max(sp.dmin[1], 1);
       load_history(h, sm, sp, t0, L < kRound ? L : kRound, dmax);
-      visit_tile(sm, sp, v0, nv, t0, L, dmax, h, more ? &B.scns[ntl.x] : nullptr, ntl.y, nx);
+      visit_tile(sm, sp, v0, nv, t0, L, dmax, h, more ? &scn_of(ntl.x) : nullptr, ntl.y, nx);
       unstage_tile(sm, sp, v0);
       __syncthreads();  // the last round's regularisation terms are in part[]
       if ((int)threadIdx.x < L)
