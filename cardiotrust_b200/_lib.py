@@ -95,6 +95,7 @@ EXPORTED = [
     "ct_scenario_dims",
     "ct_run_epoch",
     "ct_run_epoch_plain",
+    "ct_run_epoch_host",
     "ct_batch_create",
     "ct_batch_destroy",
     "ct_batch_run_epoch",
@@ -250,6 +251,8 @@ def load(path: pathlib.Path = LIB_PATH) -> ctypes.CDLL:
     lib.ct_scenario_dims.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int64)] * 4
     lib.ct_run_epoch.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), _ip, ctypes.c_int, ctypes.c_int]
     lib.ct_run_epoch_plain.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), _ip]
+    lib.ct_run_epoch_host.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), _ip, ctypes.c_int, ctypes.c_int, _fp, _fp,
+                                      _ip, _fp, _fp]
     lib.ct_batch_create.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     lib.ct_batch_destroy.argtypes = [vp]
     lib.ct_batch_run_epoch.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]

@@ -241,6 +241,31 @@ class EpochEngine:
             self.sync()
         return bi.value
 
+    def run_epoch_host(self, batch_index: int, gains: np.ndarray, coefs: np.ndarray, delays: np.ndarray,
+                       measurements: Optional[np.ndarray] = None, loss_batch: Optional[np.ndarray] = None,
+                       beat_order=None, grad_mode=GradMode.Reference, precision=DEFAULT_PRECISION) -> int:
+        """One epoch with the model in host memory, like the reference's ``run_epoch`` updating
+        ``results.model`` in place (ct_run_epoch_host): ``gains`` [S,78], ``coefs`` [V,26] and ``delays``
+        [V,26] (reference order, C-contiguous; pinned for full speed) are copied in and overwritten with
+        the updated parameters; ``measurements`` [B,T,M] (optional) is copied in; ``loss_batch``
+        [num_batch_slots] (optional) receives the batch-wise loss. One wait, at the end."""
+        D = self.dims
+        for name, arr, dtype, shape in (("gains", gains, np.float32, (D["S"], 78)), ("coefs", coefs, np.float32, (D["V"], 26)),
+                                        ("delays", delays, np.int32, (D["V"], 26)),
+                                        ("measurements", measurements, np.float32, (D["B"], D["T"], D["M"])),
+                                        ("loss_batch", loss_batch, np.float32, (D["NB"],))):
+            if arr is None and name in ("measurements", "loss_batch"):
+                continue
+            if arr.shape != shape or arr.dtype != np.dtype(dtype) or not arr.flags.c_contiguous:
+                raise CtError(_lib.CT_ERR_INVALID_ARGUMENT, f"{name} needs a C-contiguous {np.dtype(dtype)} array of shape {shape}")
+        bi = ctypes.c_int64(int(batch_index))
+        order = None if beat_order is None else _i32(beat_order)
+        check(lib().ct_run_epoch_host(self._h, ctypes.byref(bi), None if order is None else iptr(order), int(grad_mode),
+                                      int(precision), fptr(gains), fptr(coefs), iptr(delays),
+                                      None if measurements is None else fptr(measurements),
+                                      None if loss_batch is None else fptr(loss_batch)))
+        return bi.value
+
     def run_epoch_plain(self, batch_index: int = 0, beat_order=None, sync: bool = True) -> int:
         """The plain GPU form of :meth:`run_epoch` (reference gradients, FP32): one kernel launch per
         phase per step, one scenario at a time - the baseline the persistent form is measured against."""

@@ -80,6 +80,7 @@ struct ct_scn {
   // field transfers: device perm and a staging buffer of S * 78 words (voxel reordering on the device)
   int32_t* perm_dev = nullptr;
   uint32_t* xfer = nullptr;
+  uint32_t* xfer_epoch = nullptr;  // [S*78 + 2*V*26] staging of ct_run_epoch_host (gains, coefs, delays)
   // ct_calculate_final: grid types and numbers [2, cells], threshold histogram, results (grown on demand)
   int64_t final_cells = 0;
   int32_t* final_grid = nullptr;
@@ -1222,6 +1223,67 @@ int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, i
 
 int ct_run_epoch_plain(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order) {
   return run_epoch_impl(scn, batch_index, beat_order, CT_GRAD_REFERENCE, CT_PREC_FP32, true);
+}
+
+// One epoch for a caller that keeps the model in host memory, as the reference's run_epoch
+// (src/core/algorithm.rs:124-129) mutates `results.model` in place: every copy, reordering kernel
+// and the epoch go onto the context stream back to back, and the call waits once at the end.
+int ct_run_epoch_host(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, int grad_mode, int precision,
+                      float* gains, float* coefs, int32_t* delays, const float* measurements, float* loss_batch) {
+  if (!scn || !batch_index || !gains || !coefs || !delays) return fail(CT_ERR_INVALID_ARGUMENT, "NULL argument");
+  CT_DEVICE_SCOPE(scn->ctx->device);
+  DeviceScenario& d = scn->d;
+  cudaStream_t st = scn->ctx->stream;
+  // the delays of connected pairs must be >= 1, as ct_write_field checks; their largest sizes the
+  // adjoint's inbox ring
+  const std::vector<int32_t>& nbr = scn->nbr_host;
+  int64_t dmax = 1;
+  for (size_t i = 0; i < nbr.size(); ++i) {
+    if (nbr[i] < 0) continue;
+    if (delays[i] < 1)
+      return fail(CT_ERR_INVALID_ARGUMENT, "delay %zu of a connected pair is %d; delays must be >= 1", i, delays[i]);
+    if (delays[i] > dmax) dmax = delays[i];
+  }
+  int rc = ensure_xfer(scn);
+  if (rc) return rc;
+  const int64_t ng = d.S * kGainCols, nc = d.V * kOffsets;
+  if (!scn->xfer_epoch) {
+    rc = alloc(scn, &scn->xfer_epoch, ng + 2 * nc);
+    if (rc) return rc;
+  }
+  uint32_t* sg = scn->xfer_epoch;
+  uint32_t* sc = sg + ng;
+  uint32_t* sd = sc + nc;
+  // inputs: host -> staging -> device voxel order
+  CT_CUDA(cudaMemcpyAsync(sg, gains, sizeof(float) * ng, cudaMemcpyHostToDevice, st), "copy gains");
+  CT_CUDA(ct::launch_permute_blocks(sg, d.gains, scn->perm_dev, d.V, 3 * kGainCols, true, st), "permute kernel");
+  CT_CUDA(cudaMemcpyAsync(sc, coefs, sizeof(float) * nc, cudaMemcpyHostToDevice, st), "copy coefs");
+  CT_CUDA(ct::launch_permute_blocks(sc, d.coefs, scn->perm_dev, d.V, kOffsets, true, st), "permute kernel");
+  CT_CUDA(cudaMemcpyAsync(sd, delays, sizeof(int32_t) * nc, cudaMemcpyHostToDevice, st), "copy delays");
+  CT_CUDA(ct::launch_permute_blocks(sd, d.delays, scn->perm_dev, d.V, kOffsets, true, st), "permute kernel");
+  if (measurements)
+    CT_CUDA(cudaMemcpyAsync(d.meas, measurements, sizeof(float) * d.B * d.T * d.M, cudaMemcpyHostToDevice, st),
+            "copy measurements");
+  CT_CUDA(ct::launch_min_delay(d, st), "min delay kernel");
+  scn->launches += 4;
+  scn->dmax_bound = dmax;
+  scn->updates_at_read = -1;
+  rc = ct_run_epoch(scn, batch_index, beat_order, grad_mode, precision);
+  if (rc) {
+    cudaStreamSynchronize(st);
+    return rc;
+  }
+  // outputs: device voxel order -> staging -> host (the same arrays, updated in place)
+  CT_CUDA(ct::launch_permute_blocks(d.gains, sg, scn->perm_dev, d.V, 3 * kGainCols, false, st), "permute kernel");
+  CT_CUDA(cudaMemcpyAsync(gains, sg, sizeof(float) * ng, cudaMemcpyDeviceToHost, st), "copy gains");
+  CT_CUDA(ct::launch_permute_blocks(d.coefs, sc, scn->perm_dev, d.V, kOffsets, false, st), "permute kernel");
+  CT_CUDA(cudaMemcpyAsync(coefs, sc, sizeof(float) * nc, cudaMemcpyDeviceToHost, st), "copy coefs");
+  CT_CUDA(ct::launch_permute_blocks(d.delays, sd, scn->perm_dev, d.V, kOffsets, false, st), "permute kernel");
+  CT_CUDA(cudaMemcpyAsync(delays, sd, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, st), "copy delays");
+  scn->launches += 3;
+  if (loss_batch)
+    CT_CUDA(cudaMemcpyAsync(loss_batch, d.loss_b, sizeof(float) * d.NB, cudaMemcpyDeviceToHost, st), "copy loss");
+  return ct_sync(scn);
 }
 
 int ct_simulate(ct_scn* scn, float* measurements_out, float* states_out) {

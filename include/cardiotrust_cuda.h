@@ -6,6 +6,7 @@
  * (paths relative to the crate root):
  *
  *   ct_run_epoch          <- run_epoch                    src/core/algorithm.rs:124-129
+ *   ct_run_epoch_host     <- run_epoch, model in host memory (copies in, epoch, copies out)
  *                            EpochKernel::execute         src/core/algorithm/gpu/epoch.rs:96-117
  *   ct_scenario_create    <- Results::to_gpu              src/core/scenario/results.rs:121-133
  *                            EpochKernel::new             src/core/algorithm/gpu/epoch.rs:29-37
@@ -212,6 +213,18 @@ int ct_run_epoch(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, i
  * batched forms are measured against. Same arguments, results (within tolerance) and error
  * behaviour as ct_run_epoch. */
 int ct_run_epoch_plain(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order);
+
+/* ct_run_epoch for a caller that keeps the model in host memory, as the reference's
+ * run_epoch(results, batch_index, data, config) (src/core/algorithm.rs:124-129) updates
+ * `results.model` in place: gains [S,78], coefs [V,26] and delays [V,26] (reference order) are
+ * copied in, the epoch runs, and the updated arrays are copied back into the same buffers;
+ * measurements [B,T,M] (or NULL: keep the device copy) are copied in, loss_batch [num_batch_slots]
+ * (or NULL) receives the batch-wise loss (results.metrics.loss_batch). Delays of connected pairs
+ * must be >= 1 (CT_ERR_INVALID_ARGUMENT, nothing copied). All copies, the reordering kernels and the
+ * epoch are enqueued on the context stream back to back and the call waits once, at the end
+ * (device-side failures reported as by ct_sync). Pinned host memory gives full copy bandwidth. */
+int ct_run_epoch_host(ct_scn* scn, int64_t* batch_index, const int32_t* beat_order, int grad_mode, int precision,
+                      float* gains, float* coefs, int32_t* delays, const float* measurements, float* loss_batch);
 
 /* ---- batched scenarios (no counterpart in the reference, which runs one scenario per OS
  * thread, src/core/scheduler.rs:93).

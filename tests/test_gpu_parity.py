@@ -383,3 +383,39 @@ def _mr_history(o64, scn):
     H = scn.measurement_matrix[-1].astype(np.float64)
     r = o64.measurements[-1].astype(np.float64) - scn.measurements[-1].astype(np.float64)
     return r @ H
+
+
+def test_run_epoch_host_matches_device_path(alg, ctx, cuboid8):
+    """ct_run_epoch_host (model in host memory, copied in and back every epoch, one wait) gives the
+    same parameters and batch-wise losses, bit for bit, as writing the fields, running ct_run_epoch
+    and reading them back; over three epochs the host arrays carry the model forward."""
+    import torch
+
+    cfg = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-2, freeze_delays=False)
+    ref = alg.EpochEngine.from_scenario(ctx, cuboid8, num_batch_slots=3, algorithm=cfg)
+    eng = alg.EpochEngine.from_scenario(ctx, cuboid8, num_batch_slots=3, algorithm=cfg)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    gains, coefs, delays = pin(ref.read("gains")), pin(ref.read("coefs")), pin(ref.read("delays"))
+    meas = pin(cuboid8.measurements)
+    loss = pin(np.zeros(eng.dims["NB"], np.float32))
+    bi_ref = bi = 0
+    for _ in range(3):
+        bi_ref = ref.run_epoch(bi_ref, beat_order=[0], sync=True)
+        bi = eng.run_epoch_host(bi, gains, coefs, delays, meas, loss, beat_order=[0])
+    assert bi == bi_ref == 3
+    assert_bitwise(gains, ref.read("gains"), "gains")
+    assert_bitwise(coefs, ref.read("coefs"), "coefs")
+    assert np.array_equal(delays, ref.read("delays"))
+    assert_bitwise(loss, ref.read("loss_batch"), "loss_batch")
+    # a connected pair with delay 0 is refused before anything is copied
+    bad = delays.copy()
+    osi = cuboid8.model.output_state_indices
+    v, n = np.argwhere(osi[0::3, 0::3] >= 0)[0]
+    bad[v, n] = 0
+    before = gains.copy()
+    with pytest.raises(alg.CtError) as err:
+        eng.run_epoch_host(bi, gains, coefs, bad, meas, loss, beat_order=[0])
+    assert err.value.status == alg._lib.CT_ERR_INVALID_ARGUMENT
+    assert_bitwise(gains, before, "gains after a refused call")
+    ref.close()
+    eng.close()
