@@ -388,7 +388,8 @@ def _mr_history(o64, scn):
 def test_run_epoch_host_matches_device_path(alg, ctx, cuboid8):
     """ct_run_epoch_host (model in host memory, copied in and back every epoch, one wait) gives the
     same parameters and batch-wise losses, bit for bit, as writing the fields, running ct_run_epoch
-    and reading them back; over three epochs the host arrays carry the model forward."""
+    and reading them back; over three epochs (reference, adjoint, reference gradients) the host
+    arrays carry the model forward."""
     import torch
 
     cfg = alg.Algorithm(optimizer=alg.Optimizer.Adam, learning_rate=1e-2, freeze_delays=False)
@@ -399,9 +400,9 @@ def test_run_epoch_host_matches_device_path(alg, ctx, cuboid8):
     meas = pin(cuboid8.measurements)
     loss = pin(np.zeros(eng.dims["NB"], np.float32))
     bi_ref = bi = 0
-    for _ in range(3):
-        bi_ref = ref.run_epoch(bi_ref, beat_order=[0], sync=True)
-        bi = eng.run_epoch_host(bi, gains, coefs, delays, meas, loss, beat_order=[0])
+    for mode in (alg.GradMode.Reference, alg.GradMode.Adjoint, alg.GradMode.Reference):
+        bi_ref = ref.run_epoch(bi_ref, beat_order=[0], grad_mode=mode, sync=True)
+        bi = eng.run_epoch_host(bi, gains, coefs, delays, meas, loss, beat_order=[0], grad_mode=mode)
     assert bi == bi_ref == 3
     assert_bitwise(gains, ref.read("gains"), "gains")
     assert_bitwise(coefs, ref.read("coefs"), "coefs")
