@@ -56,6 +56,7 @@ def test_null_arguments_are_rejected(lib):
 
     assert lib.ct_ctx_create(0, None, None) == _lib.CT_ERR_INVALID_ARGUMENT
     assert lib.ct_run_epoch(None, None, None, 0, 0) == _lib.CT_ERR_INVALID_ARGUMENT
+    assert lib.ct_run_epoch_host(None, None, None, 0, 0, None, None, None, None, None) == _lib.CT_ERR_INVALID_ARGUMENT
     assert lib.ct_sync(None) == _lib.CT_ERR_INVALID_ARGUMENT
     buf = ctypes.create_string_buffer(256)
     assert lib.ct_last_error(buf, len(buf)) == 0
