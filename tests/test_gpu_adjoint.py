@@ -4,7 +4,7 @@ test_adjoint_oracle.py.
 
 Bars: states, measurements and metrics as in the reference mode (the
 forward is shared); gradients <= 1e-3 relative (norm-wise) to the float64
-oracle, the north-star tolerance."""
+oracle, the stated gradient tolerance."""
 
 import numpy as np
 import pytest

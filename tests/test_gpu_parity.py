@@ -5,7 +5,7 @@ Bars, written per check:
   * derivatives given the same mapped residuals: bit-identical;
   * the measurement products (H x, H^T r) sum in a different order than
     ndarray/matrixmultiply, so everything downstream of them is compared with
-    <= 1e-4 relative on states/measurements/losses,
+    the stated tolerances: <= 1e-4 relative on states/measurements/losses,
     <= 1e-3 relative (norm-wise) on gradients and parameter updates.
 """
 

@@ -2,7 +2,7 @@
 
 Bars: states bit-identical in the first epoch (same operations, same order);
 H^T r bit-identical given the same residuals is not claimed (H x reduces in a
-tree), so downstream values use the north-star tolerances."""
+tree), so downstream values use the stated tolerances (1e-4 states and losses, 1e-3 gradients)."""
 
 import numpy as np
 import pytest

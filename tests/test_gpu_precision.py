@@ -4,7 +4,7 @@ residuals are about 1 % of the signal.
 
 Here the gradient is a near-cancelling sum of small residual terms. A product whose error leans one
 way (the tensor core's FP32 accumulation loses low bits toward zero) biases it, while unbiased rounding
-averages out. The bar is the north star's: every gradient within 1e-3 (norm-wise relative) of the f64
+averages out. The bar is the stated gradient tolerance: every gradient within 1e-3 (norm-wise relative) of the f64
 oracle, in both gradient modes, for the FP32 CUDA-core products and the sliced BF16 tensor-core products.
 The beat is cut from 8,000 to 1,000 steps so that the f64 oracle (OpenMP) finishes in a few minutes; the
 states stay bit-identical to the f32 oracle regardless.
