@@ -32,8 +32,8 @@
 //   * Pipeline. Sixteen threads (half a warp) own one voxel of the tile, five
 //     of its 78 columns each. A step's inbox row and q row (contiguous per
 //     tile; plane pitch padded to 16 bytes) arrive by TMA bulk copies into a
-//     ring of NS shared-memory stages (3, or 4 for a batch), issued NS steps ahead by one
-//     thread and completed on a `full` mbarrier per stage; the states, mapped
+//     ring of NS shared-memory stages (3, or 4 for a batch), issued NS steps
+//     ahead by one thread and completed on a `full` mbarrier per stage; the states, mapped
 //     residuals and in1 gathers of the step arrive by cp.async. Warps run
 //     decoupled: each releases a stage on an `empty` mbarrier, and no CTA
 //     barrier separates steps. Every wait is bounded.
@@ -68,14 +68,14 @@ static_assert(kGroup == 16 && kCols == 5 && 4 * kGroup < kGainCols, "the inbox s
 template <int NS>
 struct AdjSmem {
   float g[kTileVoxels * 3 * kGainCols];  // the tile's gain rows, [voxel][row a][column k] as in HBM
-  float stage[NS][3][kTileCols];    // [stage][inbox | q | in1][voxel * 78 + column]
-  float xm[NS][kTileVoxels][8];     // [stage][voxel][x0 x1 x2 mr0 mr1 mr2 - -]
+  float stage[NS][3][kTileCols];         // [stage][inbox | q | in1][voxel * 78 + column]
+  float xm[NS][kTileVoxels][8];          // [stage][voxel][x0 x1 x2 mr0 mr1 mr2 - -]
   float coef[kTileItems];                // per (voxel, offset) of the tile
   int32_t del[kTileItems];
   int32_t nbr[kTileItems];
   float lam[kTileCols];                  // adjoint state carried between blocks (tiles that are not resident)
-  uint64_t full[NS];                // the stage's rows have landed
-  uint64_t empty[NS];               // every warp is done with the stage
+  uint64_t full[NS];                     // the stage's rows have landed
+  uint64_t empty[NS];                    // every warp is done with the stage
   uint64_t meta_bar;
   int abort;
   AdjScn sp;                             // scenario of the current tile
@@ -373,7 +373,7 @@ __device__ __forceinline__ bool backward_block(Cols& cs, AdjSmem<NS>& sm, const 
     cs.full_ph ^= 1u << st;
     cs.inflight &= ~(1u << st);
     cp_async_wait<NS - 1>();  // this thread's copies of step t
-    __syncwarp();                  // the voxel group's copies of step t
+    __syncwarp();             // the voxel group's copies of step t
     // lx[t] of the voxel: instantaneous terms + its 78 inbox cells (partial sums per component,
     // reduced over the 16-thread group in a fixed order)
     // column k = q + 16 i has component b = (q + i) mod 3 (16 = 1 mod 3): sum the columns i = j,
